@@ -1,0 +1,344 @@
+"""Python binding of the C ABI in include/bbtc_gpu.h (libbbtc.so).
+
+The objects mirror the reference's driver sequence (src/bbtc.cu:28-89):
+
+    st    = Graph.upload(ctx, csr, cuts)       # BlockCSR(cuts, x_adj, adj)
+    tl    = st.task_list(sorted=True)          # tasks::TaskList + SortTasks
+    bbtc  = BBTc(st, tl)                       # BBTc(&st, tasks, P)
+    bbtc.Separator = -1                        # --border
+    n     = bbtc.NoOfTriangles()               # exact u64 count
+
+Every failing C call raises :class:`BBTcError` with the library's message.
+There is no CPU path: without libbbtc.so or a B200 the calls fail.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+c = ctypes
+
+STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_INPUT", -5: "ERR_TIMEOUT",
+          -6: "ERR_NODEV", -7: "ERR_UNSUPPORTED", -8: "ERR_STATE", -9: "ERR_CAPACITY"}
+
+MODE_PERSISTENT, MODE_PLAIN = 0, 1
+KERNEL_AUTO, KERNEL_BITMAP, KERNEL_SEARCH, KERNEL_MERGE = 0, 1, 2, 3
+KERNELS = {"auto": KERNEL_AUTO, "bitmap": KERNEL_BITMAP, "search": KERNEL_SEARCH, "merge": KERNEL_MERGE}
+MODES = {"persistent": MODE_PERSISTENT, "plain": MODE_PLAIN}
+
+
+class BBTcError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+class Task(c.Structure):
+    _fields_ = [("ab", c.c_uint32), ("bc", c.c_uint32), ("ac", c.c_uint32)]
+
+
+class Opts(c.Structure):
+    _fields_ = [("mode", c.c_int), ("kernel", c.c_int), ("bitmap_words", c.c_uint32),
+                ("warps_per_block", c.c_uint32), ("unit_work", c.c_uint32), ("blocks_per_sm", c.c_uint32),
+                ("use_cuda_graph", c.c_int), ("sort_tasks", c.c_int)]
+
+
+class GraphInfo(c.Structure):
+    _fields_ = [("n", c.c_uint32), ("P", c.c_uint32), ("m", c.c_uint64), ("device_bytes", c.c_uint64),
+                ("layout_ms", c.c_double)]
+
+
+TASK_DTYPE = np.dtype([("ab", np.uint32), ("bc", np.uint32), ("ac", np.uint32)])
+
+_typed = False
+
+
+def lib() -> ctypes.CDLL:
+    global _typed
+    L = _lib._load("libbbtc.so")
+    if _typed:
+        return L
+    vp, u32, u64, i32 = c.c_void_p, c.c_uint32, c.c_uint64, c.c_int32
+    sig = {
+        "bbtc_last_error": [c.c_char_p, c.c_size_t],
+        "bbtc_version": [],
+        "bbtc_ctx_create": [c.c_int, c.POINTER(vp)],
+        "bbtc_ctx_destroy": [vp],
+        "bbtc_ctx_stream": [vp, c.POINTER(vp)],
+        "bbtc_ctx_sm_count": [vp, c.POINTER(c.c_int)],
+        "bbtc_graph_upload": [vp, u32, vp, vp, u64, vp, u32, c.POINTER(vp)],
+        "bbtc_graph_upload_device": [vp, u32, vp, vp, u64, vp, u32, c.POINTER(vp)],
+        "bbtc_graph_free": [vp],
+        "bbtc_graph_info_get": [vp, c.POINTER(GraphInfo)],
+        "bbtc_graph_tile_stats": [vp, vp, vp, vp, vp, vp],
+        "bbtc_task_list": [u32, vp, u32, c.POINTER(u32)],
+        "bbtc_sort_tasks": [vp, vp, u32, c.c_int],
+        "bbtc_count": [vp, vp, vp, u32, i32, c.POINTER(Opts), c.POINTER(u64)],
+        "bbtc_count_async": [vp, vp, vp, u32, i32, c.POINTER(Opts)],
+        "bbtc_count_wait": [vp, vp, c.POINTER(u64)],
+        "bbtc_last_launches": [vp, c.POINTER(u32)],
+        "bbtc_count_batch": [vp, vp, u32, c.POINTER(Opts), vp],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = c.c_int
+    L.bbtc_opts_default.argtypes = [c.POINTER(Opts)]
+    L.bbtc_opts_default.restype = None
+    _typed = True
+    return L
+
+
+def last_error() -> str:
+    buf = c.create_string_buffer(1024)
+    lib().bbtc_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise BBTcError(rc, last_error())
+
+
+def options(mode: str | int = "persistent", kernel: str | int = "auto", bitmap_words: int = 0,
+            warps_per_block: int = 0, unit_work: int = 0, blocks_per_sm: int = 0, cuda_graph: bool = True,
+            sort_tasks: bool = True) -> Opts:
+    o = Opts()
+    lib().bbtc_opts_default(c.byref(o))
+    o.mode = MODES[mode] if isinstance(mode, str) else int(mode)
+    o.kernel = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+    if bitmap_words:
+        o.bitmap_words = bitmap_words
+    if warps_per_block:
+        o.warps_per_block = warps_per_block
+    if unit_work:
+        o.unit_work = unit_work
+    o.blocks_per_sm = blocks_per_sm
+    o.use_cuda_graph = 1 if cuda_graph else 0
+    o.sort_tasks = 1 if sort_tasks else 0
+    return o
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+class Context:
+    """A device + stream (bbtc_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._h = c.c_void_p()
+        check(lib().bbtc_ctx_create(device, c.byref(self._h)))
+        self.device = device
+
+    @property
+    def handle(self) -> c.c_void_p:
+        if not self._h:
+            raise BBTcError(-8, "context is closed")
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        s = c.c_void_p()
+        check(lib().bbtc_ctx_stream(self.handle, c.byref(s)))
+        return s.value or 0
+
+    @property
+    def sm_count(self) -> int:
+        v = c.c_int()
+        check(lib().bbtc_ctx_sm_count(self.handle, c.byref(v)))
+        return v.value
+
+    def close(self) -> None:
+        if self._h:
+            lib().bbtc_ctx_destroy(self._h)
+            self._h = c.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """A device-resident block CSR (bbtc_graph): the reference's BlockCSR."""
+
+    def __init__(self, ctx: Context, handle: c.c_void_p, n: int, m: int, cuts: np.ndarray):
+        self.ctx = ctx
+        self._h = handle
+        self.n, self.m = n, m
+        self.cuts = cuts
+        self.P = len(cuts) - 1
+
+    @classmethod
+    def upload(cls, ctx: Context, n: int, indptr, indices, cuts) -> "Graph":
+        """Host CSR -> device block CSR (bbtc_graph_upload)."""
+        indptr, indices, cuts = _u32(indptr), _u32(indices), _u32(cuts)
+        if indptr.shape[0] != n + 1:
+            raise ValueError("indptr must have n+1 entries")
+        h = c.c_void_p()
+        check(lib().bbtc_graph_upload(ctx.handle, n, indptr.ctypes.data, indices.ctypes.data if indices.size else None,
+                                      indices.size, cuts.ctypes.data, len(cuts) - 1, c.byref(h)))
+        return cls(ctx, h, n, int(indices.size), cuts)
+
+    @classmethod
+    def upload_ptrs(cls, ctx: Context, n: int, indptr_ptr: int, indices_ptr: int, m: int, cuts) -> "Graph":
+        """Host CSR given as raw host pointers (e.g. pinned buffers) -> device block CSR."""
+        cuts = _u32(cuts)
+        h = c.c_void_p()
+        check(lib().bbtc_graph_upload(ctx.handle, n, indptr_ptr, indices_ptr, m, cuts.ctypes.data, len(cuts) - 1,
+                                      c.byref(h)))
+        return cls(ctx, h, n, m, cuts)
+
+    @classmethod
+    def upload_device(cls, ctx: Context, n: int, d_indptr: int, d_indices: int, m: int, cuts) -> "Graph":
+        """Device CSR (raw device pointers) -> device block CSR."""
+        cuts = _u32(cuts)
+        h = c.c_void_p()
+        check(lib().bbtc_graph_upload_device(ctx.handle, n, d_indptr, d_indices, m, cuts.ctypes.data,
+                                             len(cuts) - 1, c.byref(h)))
+        return cls(ctx, h, n, m, cuts)
+
+    @classmethod
+    def from_csr(cls, ctx: Context, csr, cuts) -> "Graph":
+        return cls.upload(ctx, csr.n, csr.indptr, csr.indices, cuts)
+
+    @property
+    def handle(self) -> c.c_void_p:
+        if not self._h:
+            raise BBTcError(-8, "graph is freed")
+        return self._h
+
+    def info(self) -> GraphInfo:
+        i = GraphInfo()
+        check(lib().bbtc_graph_info_get(self.handle, c.byref(i)))
+        return i
+
+    def tile_stats(self) -> dict:
+        T = self.P * self.P
+        nnz = np.zeros(T, np.uint32)
+        h = np.zeros(T, np.uint32)
+        w = np.zeros(T, np.uint32)
+        deg = np.zeros(T, np.float32)
+        mx = np.zeros(T, np.uint32)
+        check(lib().bbtc_graph_tile_stats(self.handle, nnz.ctypes.data, h.ctypes.data, w.ctypes.data,
+                                          deg.ctypes.data, mx.ctypes.data))
+        return dict(nnz=nnz, height=h, width=w, tile_deg=deg, max_deg=mx)
+
+    def task_list(self, sorted: bool = True, descending: bool = True) -> np.ndarray:
+        t = task_list(self.P)
+        if sorted:
+            check(lib().bbtc_sort_tasks(self.handle, t.ctypes.data, len(t), 1 if descending else 0))
+        return t
+
+    def count(self, tasks: np.ndarray | None = None, border: int = -1, opts: Opts | None = None) -> int:
+        out = c.c_uint64()
+        tp, nt = _tasks_arg(tasks)
+        check(lib().bbtc_count(self.ctx.handle, self.handle, tp, nt, border, c.byref(opts) if opts else None,
+                               c.byref(out)))
+        return out.value
+
+    def count_async(self, tasks: np.ndarray | None = None, border: int = -1, opts: Opts | None = None) -> None:
+        tp, nt = _tasks_arg(tasks)
+        check(lib().bbtc_count_async(self.ctx.handle, self.handle, tp, nt, border, c.byref(opts) if opts else None))
+
+    def count_wait(self) -> int:
+        out = c.c_uint64()
+        check(lib().bbtc_count_wait(self.ctx.handle, self.handle, c.byref(out)))
+        return out.value
+
+    def last_launches(self) -> int:
+        v = c.c_uint32()
+        check(lib().bbtc_last_launches(self.handle, c.byref(v)))
+        return v.value
+
+    def free(self) -> None:
+        if self._h:
+            lib().bbtc_graph_free(self._h)
+            self._h = c.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _tasks_arg(tasks):
+    if tasks is None:
+        return None, 0
+    t = np.ascontiguousarray(tasks, dtype=TASK_DTYPE)
+    return t.ctypes.data, len(t)
+
+
+def task_list(P: int) -> np.ndarray:
+    """tasks::TaskList(P): (i <= j <= k) -> (ij, jk, ik) tile ids."""
+    nt = c.c_uint32()
+    check(lib().bbtc_task_list(P, None, 0, c.byref(nt)))
+    t = np.zeros(nt.value, dtype=TASK_DTYPE)
+    check(lib().bbtc_task_list(P, t.ctypes.data, nt.value, c.byref(nt)))
+    return t
+
+
+def count_batch(ctx: Context, graphs: list[Graph], opts: Opts | None = None) -> list[int]:
+    arr = (c.c_void_p * len(graphs))(*[g.handle for g in graphs])
+    outs = np.zeros(len(graphs), dtype=np.uint64)
+    check(lib().bbtc_count_batch(ctx.handle, arr, len(graphs), c.byref(opts) if opts else None,
+                                 outs.ctypes.data))
+    return [int(x) for x in outs]
+
+
+class BBTc:
+    """The reference's driver object (include/triangle_counting/bb_tc.h:28-218)
+    over the device layout: same method names, GPU only."""
+
+    def __init__(self, st: Graph, tasks: np.ndarray | None = None, P: int | None = None):
+        if P is not None and P != st.P:
+            raise ValueError("P does not match the graph's cut vector")
+        self.st = st
+        self.tasks = st.task_list(sorted=True) if tasks is None else np.ascontiguousarray(tasks, TASK_DTYPE)
+        self.Separator = -1
+        self.opts = options()
+        self._ngpu = 1
+
+    # InitFlags / ResetFlags / PrepareGpu / CopyTilesToGpu have nothing to do:
+    # the queue lives on the device and the tiles are resident after upload.
+    def InitFlags(self) -> None:
+        pass
+
+    def ResetFlags(self) -> None:
+        pass
+
+    def PrepareGpu(self) -> None:
+        pass
+
+    def CopyTilesToGpu(self) -> None:
+        pass
+
+    def SetNGPU(self, n: int) -> None:
+        if n != 1:
+            raise BBTcError(-7, "only one GPU is served (--ngpu 1)")
+        self._ngpu = n
+
+    def GetNGPU(self) -> int:
+        return self._ngpu
+
+    def NoOfTriangles(self) -> int:
+        border = -1 if self.Separator is None or self.Separator < 0 or self.Separator >= len(self.tasks) \
+            else int(self.Separator)
+        return self.st.count(self.tasks, border, self.opts)
+
+    def CleanUp(self) -> None:
+        self.st.free()

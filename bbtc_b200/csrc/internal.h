@@ -1,0 +1,126 @@
+// Internal structures shared by the translation units of libbbtc.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/bbtc_gpu.h"
+
+namespace bbtc {
+
+// ---- errors ---------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define BBTC_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t e__ = (call);                             \
+    if (e__ != cudaSuccess) return ::bbtc::cuda_fail(e__, #call); \
+  } while (0)
+
+#define BBTC_TRY(call)          \
+  do {                          \
+    int rc__ = (call);          \
+    if (rc__ != BBTC_OK) return rc__; \
+  } while (0)
+
+constexpr uint32_t kMaxParts = 64;
+constexpr uint64_t kNoSegment = ~0ull;
+
+// One tile as the kernels see it: tile-local row pointers (H+1 entries, the
+// first is 0) and tile-local column ids, both 16-byte aligned.  An empty tile
+// has rp == nullptr.
+struct DevTile {
+  const uint32_t* rp;
+  const uint32_t* col;
+  uint32_t H, W, nnz, maxdeg;
+};
+
+// Kinds of work a task is run as (see count.cu).
+enum TaskKind : uint32_t {
+  kPivotBitmap = 0,  // pivot row -> shared bitmap of the column part, probes test bits
+  kPivotList = 1,    // pivot row -> sorted shared list, probes binary-search it
+  kPivotGlobal = 2,  // pivot row too long for shared memory: binary search in global memory
+};
+
+// One queued task: `rows` is the tile whose rows are the pivot vertices and
+// whose entries select the probe rows; `pivot` holds the pivot vertices' rows
+// (the set each intersection is tested against) and `probe` the rows that
+// are streamed against it.  For the v-centric order rows = CSC of ab
+// (reversed tile (j,i)), pivot = bc, probe = ac.  For the u-centric order
+// (the reference's row order) rows = ab, pivot = ac, probe = bc.
+struct DevTask {
+  DevTile rows;
+  DevTile pivot;
+  DevTile probe;
+  uint32_t kind;
+  uint32_t unit_edges;  // entries of `rows` per work unit
+  uint32_t slot;        // output counter index
+  uint32_t words;       // bitmap words the pivot part needs (ceil(W/32))
+};
+
+// A block CSR over one cut vector, for the forward or the reversed graph.
+struct BlockTiles {
+  uint32_t P = 0;
+  std::vector<uint32_t> nnz, maxdeg, nerows;  // P*P each
+  std::vector<uint64_t> rp_off, col_off;      // element offsets, kNoSegment when empty
+  uint32_t* d_rp = nullptr;                    // row-pointer pool
+  uint32_t* d_col = nullptr;                   // column pool
+  size_t rp_len = 0, col_len = 0;
+  void release();
+};
+
+struct Plan {
+  std::vector<DevTask> tasks;      // host copy
+  std::vector<uint32_t> prefix;    // unit prefix, ntasks + 1
+  DevTask* d_tasks = nullptr;
+  uint32_t* d_prefix = nullptr;
+  uint32_t total_units = 0;
+  uint32_t launches = 0;
+  cudaGraphExec_t exec = nullptr;
+  bool captured = false;
+  void release();
+};
+
+}  // namespace bbtc
+
+struct bbtc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sms = 0;
+  size_t smem_optin = 0;
+  uint32_t* d_unit_counter = nullptr;  // persistent-queue head (one word per launch slot)
+};
+
+struct bbtc_graph {
+  bbtc_ctx* ctx = nullptr;
+  uint32_t n = 0, P = 0;
+  uint64_t m = 0;
+  std::vector<uint32_t> cuts;
+  bbtc::BlockTiles fwd, rev;
+  uint64_t* d_count = nullptr;  // result slot
+  uint64_t device_bytes = 0;
+  double layout_ms = 0;
+  uint32_t last_launches = 0;
+  std::map<std::string, std::unique_ptr<bbtc::Plan>> plans;  // cached queues keyed by request
+};
+
+namespace bbtc {
+
+// layout.cu
+int build_layout(bbtc_graph* g, const uint32_t* d_indptr, const uint32_t* d_indices);
+DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_t x, uint32_t y);
+
+// count.cu
+int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
+                  const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o,
+                  uint64_t* d_outs, Plan* plan, bool reuse);
+int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o);
+
+}  // namespace bbtc

@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark: exact triangle counting, edges/s, on B200.
+
+Workload (N=1): R-MAT scale 22, edge factor 16, a/b/c/d = .57/.19/.19/.05,
+seed 2, symmetrised / deduplicated / degree-ordered and oriented, pal cuts,
+ncut 16 -- the single-graph B200 configuration.  A step is one exact count of
+the whole graph (every task of TaskList(16)).
+
+  value  persistent form, graph resident in HBM, device time of the count
+         (CUDA events on the library's stream), edges / second
+  plain  the same count as one launch per task (reported beside it)
+  e2e    the public C ABI from pinned host buffers: CSR upload + device layout
+         build + count + result readback, every step, wall clock
+  roofline  B_alg = 4 m + 4 sum_{(u,v)} (d+(u) + d+(v)) bytes per count over
+         the count's device time, against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own CPU path (oracle/_ref, built from its
+         sources) on the box's host cores, same graph and cuts
+
+`--impl reference` times only the reference's CPU path (all host threads).
+For N > 1 (torchrun) every rank counts its own graph of the same shape
+(seed 2 + rank): weak scaling, no collective on the data path; the counts are
+summed with one all_reduce after the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edges/sec at exact count, batched vs plain form on 1 B200; p50/p99 latency"
+UNIT = "edges/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--ncut", type=int, default=16)
+    p.add_argument("--partitioner", default="pal")
+    p.add_argument("--kernel", default="auto")
+    p.add_argument("--bitmap-words", type=int, default=0)
+    p.add_argument("--unit-work", type=int, default=0)
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-threads", type=int, default=0)
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [ln.strip().split(",") for ln in self.file.read().splitlines() if ln.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() in ("active", "1"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_traffic(scale: int, ncut: int):
+    """Per-launch DRAM bytes of the count kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_count_queue_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        key = f"rmat-s{scale}-p{ncut}"
+        return d[key]["dram_bytes_per_launch"], d[key].get("note")
+    except Exception:
+        return None, None
+
+
+def make_graph(args, seed):
+    from bbtc_b200 import graphs
+    t0 = time.time()
+    g = graphs.rmat(args.scale, args.edge_factor, seed=seed)
+    cuts = graphs.cuts(g, args.ncut, args.partitioner)
+    return g, cuts, time.time() - t0
+
+
+def run_reference(args, rank: int):
+    """Reference arm: the reference's own CPU counting path, all host threads."""
+    import oracle
+    if rank != 0:
+        return None
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libbbtc_ref.so not built"}
+    g, cuts, _ = make_graph(args, args.seed)
+    threads = args.cpu_threads or os.cpu_count()
+    count, secs = oracle.ref_count(g.n, g.indptr, g.indices, cuts, nthreads=threads,
+                                   repeat=args.warmup + args.steps)
+    timed = secs[args.warmup:]
+    t = statistics.median(timed)
+    value = g.m / t
+    sample = (f"full workload per step: NoOfTriangles() over all {args.ncut * (args.ncut + 1) * (args.ncut + 2) // 6}"
+              f" tasks, median of {len(timed)} steps after {args.warmup} warm-up")
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"rmat-s{args.scale}-ef{args.edge_factor}-seed{args.seed} {args.partitioner} "
+                               f"ncut {args.ncut}", "n": g.n, "m": g.m, "triangles": count},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        res = run_reference(args, rank)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from bbtc_b200 import Context, Graph, graphs, options
+
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    g, cuts, gen_s = make_graph(args, args.seed + rank)
+    balg = g.algorithmic_bytes()
+    st = Graph.from_csr(ctx, g, cuts)
+    layout_ms = st.info().layout_ms
+    device_bytes = st.info().device_bytes
+    o = options(mode="persistent", kernel=args.kernel, bitmap_words=args.bitmap_words, unit_work=args.unit_work,
+                cuda_graph=True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def timed_counts(opts, steps, warmup):
+        for _ in range(warmup):
+            st.count(opts=opts)
+        times, counts = [], set()
+        launches = 0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)  # evicts L2 (126 MB) between timed steps
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                st.count_async(opts=opts)
+                e1.record(stream)
+            counts.add(st.count_wait())
+            launches += st.last_launches()
+            times.append(e0.elapsed_time(e1))
+        return times, counts, launches
+
+    # --- persistent form (the headline value) ---
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    times, counts, launches = timed_counts(o, args.steps, args.warmup)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t_mean = sum(times) / len(times) / 1e3
+    assert len(counts) == 1, f"count changed between steps: {counts}"
+    count = counts.pop()
+    t_max = t_mean
+    m_total = g.m
+    if dist is not None:
+        tt = torch.tensor([t_mean], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        mm = torch.tensor([g.m, count], dtype=torch.int64, device=f"cuda:{local}")
+        dist.all_reduce(mm)
+        m_total, count_total = int(mm[0].item()), int(mm[1].item())
+    value = m_total / t_max
+
+    # --- plain form (one launch per task) ---
+    plain = None
+    if not args.no_plain:
+        po = options(mode="plain", kernel=args.kernel, bitmap_words=args.bitmap_words, unit_work=args.unit_work,
+                     cuda_graph=False)
+        ptimes, pcounts, plaunches = timed_counts(po, max(3, args.steps // 2), 2)
+        assert pcounts == {count}, f"plain form disagrees: {pcounts} vs {count}"
+        pt = sum(ptimes) / len(ptimes) / 1e3
+        plain = {"value": g.m / pt, "unit": UNIT, "ms_per_step": pt * 1e3,
+                 "launches_per_step": plaunches // len(ptimes), "persistent_over_plain": pt / t_mean}
+
+    # --- e2e through the C ABI from pinned host buffers ---
+    e2e = None
+    if not args.no_e2e:
+        ip = torch.from_numpy(g.indptr.view(np.int32)).pin_memory()
+        ix = torch.from_numpy(g.indices.view(np.int32)).pin_memory()
+        from bbtc_b200 import core
+        e2e_t = []
+        for i in range(args.warmup + max(3, args.steps // 2)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            h = core.Graph.upload_ptrs(ctx, g.n, ip.data_ptr(), ix.data_ptr(), g.m, cuts)
+            c2 = h.count(opts=o)
+            h.free()
+            t1 = time.perf_counter()
+            assert c2 == count
+            if i >= args.warmup:
+                e2e_t.append(t1 - t0)
+        te = statistics.median(e2e_t)
+        e2e = {"value": g.m / te, "unit": UNIT, "ms_per_step": te * 1e3,
+               "h2d_bytes_per_step": int(4 * (g.n + 1) + 4 * g.m + 4 * len(cuts)),
+               "d2h_bytes_per_step": 8,
+               "note": "upload (H2D from pinned memory) + device layout build + persistent count + 8-byte "
+                       "readback, wall clock; the library's control copies (tile statistics, task queue, "
+                       "< 1 MB) are not in the byte counts"}
+
+    # --- CPU baseline: the reference's own CPU path on this host ---
+    cpu = None
+    ref_match = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        import oracle
+        if oracle.ref_available():
+            threads = args.cpu_threads or os.cpu_count()
+            rc, secs = oracle.ref_count(g.n, g.indptr, g.indices, cuts, nthreads=threads, repeat=1)
+            ref_match = (rc == count)
+            cpu = {"value": g.m / secs[0], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": "the full workload once: the reference's NoOfTriangles() over all tasks of the "
+                             "same graph and cuts (oracle/_ref, built from the reference's sources)",
+                   "seconds": secs[0], "count_matches_gpu": ref_match}
+
+    peak, peak_kind = peaks()
+    achieved = balg / t_mean / 1e9
+    traffic, traffic_note = load_traffic(args.scale, args.ncut)
+    res = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"rmat-s{args.scale}-ef{args.edge_factor}-seed{args.seed} {args.partitioner} "
+                               f"ncut {args.ncut}", "n": g.n, "m": g.m, "P": args.ncut,
+                   "partitioner": args.partitioner, "mode": "persistent (one launch, device queue, CUDA graph)",
+                   "kernel": args.kernel, "triangles": count if world == 1 else count_total,
+                   "layout_ms": layout_ms, "device_bytes": device_bytes, "generate_s": round(gen_s, 2),
+                   "l2": "block CSR larger than L2, plus a 256 MiB fill between timed steps (excluded)",
+                   "parallelism": "replicas per GPU" if world > 1 else "single GPU"},
+        "plain": plain,
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes": balg,
+                     "note": ("achieved = B_alg / count time; B_alg counts the ids a merge streams, so L2 "
+                              "reuse and the bitmap's single read of each pivot row can put frac above 1"
+                              + (f"; traffic: {traffic_note}" if traffic_note else ""))},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "triangles_per_sec": (count / t_mean) if world == 1 else None,
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    st.free()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

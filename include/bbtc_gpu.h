@@ -1,0 +1,170 @@
+/*
+ * bbtc_gpu.h -- C ABI of the B200 triangle-counting path (libbbtc.so).
+ *
+ * Exact triangle counting over a 2D-partitioned block CSR, task model
+ * (i <= j <= k) as in GT-TDAlab/bbTC.  Every function returns an int status:
+ * 0 (BBTC_OK) or a negative bbtc_status; bbtc_last_error() gives the message
+ * of the calling thread's last failure.  No function exits the process.
+ *
+ * Reference interfaces each entry point replaces (paths inside the bbTC
+ * project):
+ *   - class BBTc                         include/triangle_counting/bb_tc.h:28-218
+ *   - BlockCSR(cuts, x_adj, adj)         src/data_structures/block_csr.cpp:35-42, 288-376
+ *   - tasks::TaskList / tasks::SortTasks include/utils/tasks.hpp:7-34
+ *   - DenseKernel / SparseKernel launch  src/triangle_counting/bb_tc.cpp:76-115
+ *   - BBTc::NoOfTriangles                src/triangle_counting/bb_tc.cpp:200-252
+ * Threading: a context and the graphs made with it belong to one host thread
+ * at a time (the reference drives BBTc from the main thread, src/bbtc.cu:40-89);
+ * the request server (bbtc_server_*) is safe to call from any thread.
+ */
+#ifndef BBTC_GPU_H_
+#define BBTC_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bbtc_status {
+  BBTC_OK = 0,
+  BBTC_ERR_ARG = -1,         /* bad argument (null pointer, out-of-range value) */
+  BBTC_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  BBTC_ERR_NOMEM = -3,       /* device or host allocation failed */
+  BBTC_ERR_INPUT = -4,       /* the CSR or cut vector breaks the input contract */
+  BBTC_ERR_TIMEOUT = -5,     /* a bounded device wait ran out */
+  BBTC_ERR_NODEV = -6,       /* no usable CUDA device / wrong device index */
+  BBTC_ERR_UNSUPPORTED = -7, /* valid request this build does not serve */
+  BBTC_ERR_STATE = -8,       /* call out of order (e.g. polling an unknown request) */
+  BBTC_ERR_CAPACITY = -9     /* admission refused: over the HBM budget or slot limit */
+} bbtc_status;
+
+typedef struct bbtc_ctx bbtc_ctx;
+typedef struct bbtc_graph bbtc_graph;
+
+/* Copy the calling thread's last error message (NUL-terminated, truncated). */
+int bbtc_last_error(char* buf, size_t len);
+
+/* Library version as major*10000 + minor*100 + patch. */
+int bbtc_version(void);
+
+/* ---- context: device, stream, scratch ------------------------------------
+ * Replaces BBTc's constructor GPU set-up and PrepareGpu
+ * (src/triangle_counting/bb_tc.cpp:17-33, bb_tc_helper.cpp:53-73): one
+ * stream, no per-stream global bitmap.  Only device 0..count-1 are valid;
+ * the reference's multi-GPU striping (--ngpu > 1) is not served. */
+int bbtc_ctx_create(int device, bbtc_ctx** out);
+int bbtc_ctx_destroy(bbtc_ctx* ctx);
+/* The cudaStream_t the context launches on (returned as void*). */
+int bbtc_ctx_stream(bbtc_ctx* ctx, void** stream);
+/* Number of SMs of the context's device. */
+int bbtc_ctx_sm_count(bbtc_ctx* ctx, int* sms);
+
+/* ---- graph: device-resident block CSR ------------------------------------
+ * Replaces BlockCSR(cuts, x_adj, adj) + CSRtoBCSR (block_csr.cpp:35-42,
+ * 288-376) and the lazy per-tile copies of CopyTileToGpu
+ * (bb_tc_helper.cpp:75-110).  Input contract:
+ *   - indptr[n+1], indices[m]: CSR with indptr[0] = 0, indptr[n] = m,
+ *     non-decreasing; every row strictly increasing; every id < n.
+ *     (The counting graph is the degree-ordered, oriented one; the count is
+ *     the reference's task sum for any CSR that meets this contract.)
+ *   - cuts[P+1]: cuts[0] = 0, non-decreasing, cuts[P] >= n (rows >= n are
+ *     empty, like the phantom row the reference adds, utils.hpp:288); 1 <= P <= 64.
+ * The library builds every tile's CSR and CSC on the device; segments start
+ * 16-byte aligned.  The caller keeps its buffers. */
+int bbtc_graph_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* indptr, const uint32_t* indices,
+                      uint64_t m, const uint32_t* cuts, uint32_t P, bbtc_graph** out);
+/* Same, with indptr / indices already in device memory of the context's
+ * device (cuts stay on the host).  Nothing is copied from the host. */
+int bbtc_graph_upload_device(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_indptr,
+                             const uint32_t* d_indices, uint64_t m, const uint32_t* cuts, uint32_t P,
+                             bbtc_graph** out);
+int bbtc_graph_free(bbtc_graph* g);
+
+typedef struct bbtc_graph_info {
+  uint32_t n;             /* rows (vertices) */
+  uint32_t P;             /* number of parts (the reference's --ncut) */
+  uint64_t m;             /* oriented edges, the reference's "Number of Edges" */
+  uint64_t device_bytes;  /* device memory the graph holds */
+  double layout_ms;       /* device time of the layout build */
+} bbtc_graph_info;
+int bbtc_graph_info_get(const bbtc_graph* g, bbtc_graph_info* info);
+
+/* Per-tile statistics, row-major over the P x P grid (any pointer may be
+ * NULL).  nnz / height are the reference's GetNNZ / GetHeight
+ * (block_csr.cpp:88-92, 183-186); tile_deg = nnz / height is GetTileDeg
+ * (block_csr.cpp:258-284).  max_deg = longest row of the tile. */
+int bbtc_graph_tile_stats(const bbtc_graph* g, uint32_t* nnz, uint32_t* height, uint32_t* width,
+                          float* tile_deg, uint32_t* max_deg);
+
+/* ---- tasks ----------------------------------------------------------------
+ * A task names three tiles by row-major id: ab = i*P+j, bc = j*P+k,
+ * ac = i*P+k, i <= j <= k -- the entries of tasks::TaskList (tasks.hpp:7-17). */
+typedef struct bbtc_task {
+  uint32_t ab, bc, ac;
+} bbtc_task;
+
+/* Fill the P(P+1)(P+2)/6 tasks in TaskList order.  With out == NULL only
+ * *ntasks is set; otherwise cap must hold them all. */
+int bbtc_task_list(uint32_t P, bbtc_task* out, uint32_t cap, uint32_t* ntasks);
+/* Sort by the reference weight nnz(ab) * max(tile_deg(bc), tile_deg(ac))
+ * (tasks.hpp:19-34); descending != 0 gives the CUDA build's order.  Ties keep
+ * list order (stable). */
+int bbtc_sort_tasks(const bbtc_graph* g, bbtc_task* tasks, uint32_t ntasks, int descending);
+
+/* ---- counting --------------------------------------------------------------- */
+typedef enum bbtc_mode {
+  BBTC_MODE_PERSISTENT = 0, /* one launch pulls every task's work units from a device queue */
+  BBTC_MODE_PLAIN = 1       /* one launch per task, like NoOfTrianglesInGPU (bb_tc.cpp:76-115) */
+} bbtc_mode;
+
+typedef enum bbtc_kernel {
+  BBTC_KERNEL_AUTO = 0,   /* per task: bitmap when the bc rows fit the bitmap, else search */
+  BBTC_KERNEL_BITMAP = 1, /* pivot row of bc as a shared-memory bitmap, probes from ac */
+  BBTC_KERNEL_SEARCH = 2, /* pivot row of bc as a sorted shared-memory list, binary-search probes */
+  BBTC_KERNEL_MERGE = 3   /* row of ab per warp, warp-cooperative merge/gallop of ac and bc rows */
+} bbtc_kernel;
+
+typedef struct bbtc_opts {
+  int mode;                  /* bbtc_mode */
+  int kernel;                /* bbtc_kernel */
+  uint32_t bitmap_words;     /* shared bitmap words per warp: 0 = default (2048) */
+  uint32_t warps_per_block;  /* 0 = default (8) */
+  uint32_t unit_work;        /* target probes per work unit, 0 = default */
+  uint32_t blocks_per_sm;    /* persistent grid = SMs x this, 0 = occupancy limit */
+  int use_cuda_graph;        /* replay the launch sequence through a captured CUDA graph */
+  int sort_tasks;            /* when tasks == NULL: 1 = cost-sorted descending (default) */
+} bbtc_opts;
+
+void bbtc_opts_default(bbtc_opts* o);
+
+/* Count triangles: the sum over tasks of sum_{r in ab} sum_{b in ab[r]} |ac[r] ∩ bc[b]|.
+ * tasks == NULL counts the whole TaskList(P) (sorted per opts->sort_tasks).
+ * border follows --border (utils.hpp:111-114, bbtc.cu:54-62): -1 = every task
+ * on the GPU; b >= 0 = tasks [0, b) are queued first, then the rest; all on
+ * the GPU (there are no CPU workers).  *out receives the exact count.
+ * Replaces BBTc::NoOfTriangles (bb_tc.cpp:200-252). */
+int bbtc_count(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint32_t ntasks, int32_t border,
+               const bbtc_opts* opts, uint64_t* out);
+
+/* Enqueue the same count on the context's stream without waiting; the count
+ * lands in device memory owned by the graph.  bbtc_count_wait synchronises the
+ * stream and returns it.  Used to time the device path with stream events. */
+int bbtc_count_async(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint32_t ntasks,
+                     int32_t border, const bbtc_opts* opts);
+int bbtc_count_wait(bbtc_ctx* ctx, bbtc_graph* g, uint64_t* out);
+
+/* Launches of this library's kernels issued by the last count on g. */
+int bbtc_last_launches(const bbtc_graph* g, uint32_t* launches);
+
+/* Count many graphs in one persistent launch: every graph's TaskList(P)
+ * goes into one cost-sorted device queue, each graph gets its own u64.  outs[ng]. */
+int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, const bbtc_opts* opts,
+                     uint64_t* outs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BBTC_GPU_H_ */
