@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CXX = os.environ.get("BBTC_CXX", shutil.which("g++") or "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["api.cu", "layout.cu", "count.cu"]
-HOST_SOURCES = ["graphgen.cpp", "partition.cpp"]
+HOST_SOURCES = ["graphgen.cpp", "partition.cpp", "graph_io.cpp"]
 
 
 def _run(cmd: list[str]) -> None:
@@ -73,10 +73,10 @@ def build_cli(force: bool = False) -> str | None:
         return None
     os.makedirs(BIN, exist_ok=True)
     out = os.path.join(BIN, "bbtc")
-    deps = _deps(["bbtc_cli.cpp", "graph_io.cpp"] + HOST_SOURCES)
+    deps = _deps(["bbtc_cli.cpp"] + HOST_SOURCES)
     deps = [d for d in deps if os.path.exists(d)]
     if force or _stale(out, deps + [os.path.join(LIB, "libbbtc.so")]):
-        srcs = [os.path.join(CSRC, s) for s in ["bbtc_cli.cpp", "graph_io.cpp"] + HOST_SOURCES
+        srcs = [os.path.join(CSRC, s) for s in ["bbtc_cli.cpp"] + HOST_SOURCES
                 if os.path.exists(os.path.join(CSRC, s))]
         _run([CXX, "-O3", "-fopenmp", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-o", out] + srcs
              + ["-L", LIB, "-lbbtc", "-Wl,-rpath,$ORIGIN/../lib", "-L/usr/local/cuda/lib64", "-lcudart"])

@@ -26,8 +26,9 @@ STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_INPU
           -6: "ERR_NODEV", -7: "ERR_UNSUPPORTED", -8: "ERR_STATE", -9: "ERR_CAPACITY"}
 
 MODE_PERSISTENT, MODE_PLAIN = 0, 1
-KERNEL_AUTO, KERNEL_BITMAP, KERNEL_SEARCH, KERNEL_MERGE = 0, 1, 2, 3
-KERNELS = {"auto": KERNEL_AUTO, "bitmap": KERNEL_BITMAP, "search": KERNEL_SEARCH, "merge": KERNEL_MERGE}
+KERNEL_AUTO, KERNEL_BITMAP, KERNEL_SEARCH, KERNEL_MERGE, KERNEL_FUSED = 0, 1, 2, 3, 4
+KERNELS = {"auto": KERNEL_AUTO, "bitmap": KERNEL_BITMAP, "search": KERNEL_SEARCH, "merge": KERNEL_MERGE,
+           "fused": KERNEL_FUSED}
 MODES = {"persistent": MODE_PERSISTENT, "plain": MODE_PLAIN}
 
 

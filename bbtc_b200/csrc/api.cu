@@ -70,8 +70,8 @@ std::vector<bbtc_task> default_tasks(const bbtc_graph* g, bool sorted) {
   return t;
 }
 
-int finish_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_indptr, const uint32_t* d_indices, uint64_t m,
-                  const uint32_t* cuts, uint32_t P, bbtc_graph** out) {
+int finish_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* indptr, const uint32_t* indices, uint64_t m,
+                  const uint32_t* cuts, uint32_t P, bool host, bbtc_graph** out) {
   bbtc_graph* g = new (std::nothrow) bbtc_graph();
   if (!g) return fail(BBTC_ERR_NOMEM, "host allocation failed");
   g->ctx = ctx;
@@ -84,7 +84,7 @@ int finish_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_indptr, const uin
     delete g;
     return fail(BBTC_ERR_NOMEM, "device allocation of the result slot failed");
   }
-  const int rc = build_layout(g, d_indptr, d_indices);
+  int rc = build_layout(g, indptr, indices, host);
   if (rc != BBTC_OK) {
     bbtc_graph_free(g);
     return rc;
@@ -133,6 +133,15 @@ int bbtc_ctx_create(int device, bbtc_ctx** out) {
     delete c;
     return cuda_fail(e, "cudaStreamCreateWithFlags");
   }
+  {
+    // keep freed blocks in the device's default pool: repeated uploads reuse them
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   e = cudaMalloc(&c->d_unit_counter, 64 * sizeof(uint32_t));
   if (e != cudaSuccess) {
     cudaStreamDestroy(c->stream);
@@ -174,23 +183,7 @@ int bbtc_graph_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* indptr, const u
   BBTC_TRY(validate_cuts(n, cuts, P));
   if (indptr[0] != 0 || indptr[n] != m) return fail(BBTC_ERR_INPUT, "indptr[0] must be 0 and indptr[n] must be m");
   BBTC_CUDA(cudaSetDevice(ctx->device));
-  uint32_t *d_indptr = nullptr, *d_indices = nullptr;
-  cudaError_t e1 = cudaMalloc(&d_indptr, ((size_t)n + 1) * sizeof(uint32_t));
-  cudaError_t e2 = cudaMalloc(&d_indices, std::max<uint64_t>(m, 1) * sizeof(uint32_t));
-  if (e1 != cudaSuccess || e2 != cudaSuccess) {
-    cudaGetLastError();
-    if (d_indptr) cudaFree(d_indptr);
-    if (d_indices) cudaFree(d_indices);
-    return fail(BBTC_ERR_NOMEM, "device allocation of the input CSR failed");
-  }
-  struct Free2 {
-    uint32_t *a, *b;
-    ~Free2() { cudaFree(a); cudaFree(b); }
-  } guard{d_indptr, d_indices};
-  BBTC_CUDA(cudaMemcpyAsync(d_indptr, indptr, ((size_t)n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                            ctx->stream));
-  if (m) BBTC_CUDA(cudaMemcpyAsync(d_indices, indices, m * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
-  return finish_upload(ctx, n, d_indptr, d_indices, m, cuts, P, out);
+  return finish_upload(ctx, n, indptr, indices, m, cuts, P, /*host=*/true, out);
 }
 
 int bbtc_graph_upload_device(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_indptr, const uint32_t* d_indices,
@@ -201,7 +194,7 @@ int bbtc_graph_upload_device(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_indptr
   if (n == 0xffffffffu) return fail(BBTC_ERR_ARG, "n must be below 2^32 - 1");
   BBTC_TRY(validate_cuts(n, cuts, P));
   BBTC_CUDA(cudaSetDevice(ctx->device));
-  return finish_upload(ctx, n, d_indptr, d_indices, m, cuts, P, out);
+  return finish_upload(ctx, n, d_indptr, d_indices, m, cuts, P, /*host=*/false, out);
 }
 
 int bbtc_graph_free(bbtc_graph* g) {
@@ -209,8 +202,12 @@ int bbtc_graph_free(bbtc_graph* g) {
   cudaSetDevice(g->ctx->device);
   cudaStreamSynchronize(g->ctx->stream);
   for (auto& kv : g->plans) kv.second->release();
-  g->fwd.release();
-  g->rev.release();
+  cudaStream_t s = g->ctx->stream;
+  g->fwd.release(s);
+  g->rev.release(s);
+  if (g->d_indptr) cudaFreeAsync(g->d_indptr, s);
+  if (g->d_indices) cudaFreeAsync(g->d_indices, s);
+  cudaStreamSynchronize(s);
   if (g->d_count) cudaFree(g->d_count);
   delete g;
   return BBTC_OK;
@@ -287,7 +284,7 @@ void bbtc_opts_default(bbtc_opts* o) {
   std::memset(o, 0, sizeof(*o));
   o->mode = BBTC_MODE_PERSISTENT;
   o->kernel = BBTC_KERNEL_AUTO;
-  o->bitmap_words = 2048;
+  o->bitmap_words = 1024;
   o->warps_per_block = 8;
   o->unit_work = 8192;
   o->blocks_per_sm = 0;
@@ -303,7 +300,11 @@ static int count_async_impl(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks
   bbtc_opts o;
   if (opts) o = *opts; else bbtc_opts_default(&o);
   if (o.mode != BBTC_MODE_PLAIN && o.mode != BBTC_MODE_PERSISTENT) return fail(BBTC_ERR_ARG, "unknown mode");
-  if (o.kernel < BBTC_KERNEL_AUTO || o.kernel > BBTC_KERNEL_MERGE) return fail(BBTC_ERR_ARG, "unknown kernel");
+  if (o.kernel < BBTC_KERNEL_AUTO || o.kernel > BBTC_KERNEL_FUSED) return fail(BBTC_ERR_ARG, "unknown kernel");
+  if (o.kernel == BBTC_KERNEL_FUSED && tasks)
+    return fail(BBTC_ERR_ARG, "fused task rows run the whole task list: pass tasks = NULL");
+  const bool fused = !tasks && (o.kernel == BBTC_KERNEL_FUSED ||
+                                (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT));
   BBTC_CUDA(cudaSetDevice(ctx->device));
   std::vector<std::vector<bbtc_task>> tl(1);
   if (tasks) tl[0].assign(tasks, tasks + ntasks); else tl[0] = default_tasks(g, o.sort_tasks != 0);
@@ -320,7 +321,7 @@ static int count_async_impl(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks
     }
     it = g->plans.emplace(key, std::make_unique<Plan>()).first;
   }
-  const int rc = count_enqueue(ctx, gs, tl, o, g->d_count, it->second.get(), reuse);
+  const int rc = count_enqueue(ctx, gs, tl, o, fused, g->d_count, it->second.get(), reuse);
   if (rc != BBTC_OK) {
     it->second->release();
     g->plans.erase(it);
@@ -362,6 +363,7 @@ int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, cons
   bbtc_opts o;
   if (opts) o = *opts; else bbtc_opts_default(&o);
   if (o.mode != BBTC_MODE_PERSISTENT && o.mode != BBTC_MODE_PLAIN) return fail(BBTC_ERR_ARG, "unknown mode");
+  if (o.kernel < BBTC_KERNEL_AUTO || o.kernel > BBTC_KERNEL_FUSED) return fail(BBTC_ERR_ARG, "unknown kernel");
   BBTC_CUDA(cudaSetDevice(ctx->device));
   std::vector<bbtc_graph*> gs(graphs, graphs + ng);
   std::vector<std::vector<bbtc_task>> tl(ng);
@@ -378,7 +380,8 @@ int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, cons
   Plan plan;
   o.use_cuda_graph = 0;
   // one queue for all graphs: tasks of every graph merged by cost, heaviest first
-  int rc = count_enqueue(ctx, gs, tl, o, d_outs, &plan, false);
+  const bool fused = o.kernel == BBTC_KERNEL_FUSED || (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT);
+  int rc = count_enqueue(ctx, gs, tl, o, fused, d_outs, &plan, false);
   if (rc == BBTC_OK) {
     cudaError_t e = cudaMemcpyAsync(outs, d_outs, ng * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

@@ -3,29 +3,37 @@
 // A task (i, j, k) contributes sum_{r in part i} sum_{b in ab[r]} |ac[r] ∩ bc[b]|
 // (the reference's SparseKernel / DenseKernel, src/triangle_counting/
 // gpu_sparse_kernel.cu:6-49 and gpu_dense_kernel.cu:3-47, one thread per row
-// of ab).  The same sum is taken here one *pivot row* at a time:
+// of ab).  Here the sum is taken one *pivot row* at a time: the pivot row
+// becomes a membership structure in the warp's shared memory and the rows it
+// meets are streamed against it.
 //
-//   v-centric (default): for each row b of bc (vertex v of part j), the row
-//     bc[b] becomes a membership structure in the warp's shared memory, and
-//     every u with b in ab[u] -- the CSC column b of ab, i.e. the reversed
-//     tile (j, i) -- streams its row ac[u] against it.  With the degree order
-//     the ac rows are the shorter side, so this probes sum d_k(u) ids where the
-//     reference's bitmap form probes sum d_k(v).
-//   u-centric (the reference's row order): pivot = ac[r], the rows bc[b] for
-//     b in ab[r] are streamed against it.
+// Per-task execution (plain form, explicit task lists):
+//   v-centric (default): pivot = row b of bc (vertex v of part j); the rows
+//     streamed are ac[u] for every u with b in ab[u] -- column b of ab, read
+//     from the reversed tile (j, i).  With the degree order the ac rows are the
+//     shorter side, so this probes sum d_k(u) ids where the reference's bitmap
+//     form probes sum d_k(v).
+//   u-centric (the reference's row order, BBTC_KERNEL_MERGE): pivot = ac[r],
+//     the rows bc[b] for b in ab[r] are streamed against it.
 //
-// Membership structures (TaskKind): a bitmap of the column part (when the part
-// is at most 32 * bitmap_words ids wide), a sorted copy of the pivot row
-// searched by bisection, or -- for pivot rows longer than the shared buffer --
-// bisection in global memory.
+// Fused task rows (persistent form over the whole task list): the tasks
+// (i, j, k) for all k >= j share their ab tile, and their sum over k is
+// sum_{(u, v) in ab} |N+(u) ∩ N+(v)| with every common neighbour w > v.  One
+// pass over the reversed tile (j, i) takes it: per pivot v the whole row N+(v)
+// is the structure, and per in-edge (u, v) the ids of N+(u) after v are
+// streamed -- their range is stored with the in-edge, so no row pointer is
+// chased.  This visits each edge once instead of once per k.
+//
+// Membership structures: a bitmap (of the column part, or of the pivot row's
+// id span), a sorted copy searched by bisection, or -- for pivot rows longer
+// than the shared buffer -- bisection in global memory.
 //
 // Work units are runs of `unit_edges` consecutive entries of the rows tile.
 // In the persistent form every warp of a grid sized to the SM count claims
-// units from one atomic head over all tasks (cost-sorted, heaviest first);
-// in the plain form each task is one launch whose warps stride over its units.
-// The per-probe-row work inside a unit is balanced across the 32 lanes with a
-// merge-path split: the probe rows of 32 entries are concatenated and each lane
-// takes one contiguous 1/32 of the ids.
+// units from one atomic head over all tasks (cost-sorted, heaviest first); in
+// the plain form each task is one launch whose warps stride over its units.
+// Inside a unit the rows met by 32 entries are concatenated and split into 32
+// equal contiguous slices (merge-path split), one per lane.
 #include <algorithm>
 #include <cstring>
 #include <sstream>
@@ -56,13 +64,16 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t 
 struct PivotView {
   const uint32_t* row;  // global pivot row
   uint32_t len;
+  uint32_t base;  // bitmap bit 0 <-> id `base`
+  uint32_t span;  // ids in [base, base + span) may be set
   uint32_t first, last;
 };
 
 template <uint32_t KIND>
 __device__ __forceinline__ uint32_t member(const uint32_t* bm, const PivotView& pv, uint32_t x) {
   if constexpr (KIND == kPivotBitmap) {
-    return (bm[x >> 5] >> (x & 31)) & 1u;
+    const uint32_t y = x - pv.base;
+    return y < pv.span ? (bm[y >> 5] >> (y & 31)) & 1u : 0u;
   } else if constexpr (KIND == kPivotList) {
     if (x < pv.first || x > pv.last) return 0;
     const uint32_t p = lower_bound_u32(bm, pv.len, x);
@@ -74,11 +85,29 @@ __device__ __forceinline__ uint32_t member(const uint32_t* bm, const PivotView& 
   }
 }
 
-// Probe the rows selected by entries [e, ee) of the rows tile against the
-// pivot structure; returns this lane's hit count.
-template <uint32_t KIND>
-__device__ __forceinline__ uint32_t probe_entries(const uint32_t* __restrict__ rcol, uint32_t e, uint32_t ee,
-                                                  const uint32_t* __restrict__ prb_rp,
+// Segment of the probe ids met by entry q of the rows tile.
+struct TileSegs {  // per task: the probe tile's row r = rows.col[q]
+  const uint32_t* __restrict__ rcol;
+  const uint32_t* __restrict__ rp;
+  __device__ __forceinline__ void get(uint32_t q, uint32_t& start, uint32_t& len) const {
+    const uint32_t r = rcol[q];
+    start = rp[r];
+    len = rp[r + 1] - start;
+  }
+};
+struct RecSegs {  // fused: the stored (start, end) of N+(u) after v
+  const uint2* __restrict__ rec;
+  __device__ __forceinline__ void get(uint32_t q, uint32_t& start, uint32_t& len) const {
+    const uint2 r = rec[q];
+    start = r.x;
+    len = r.y - r.x;
+  }
+};
+
+// Probe the rows met by entries [e, ee) against the pivot structure; returns
+// this lane's hit count.
+template <uint32_t KIND, class Segs>
+__device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, uint32_t ee,
                                                   const uint32_t* __restrict__ prb_col, const uint32_t* bm,
                                                   uint32_t* sstart, uint32_t* sbase, const PivotView& pv,
                                                   uint32_t lane) {
@@ -86,11 +115,7 @@ __device__ __forceinline__ uint32_t probe_entries(const uint32_t* __restrict__ r
   for (uint32_t base = e; base < ee; base += 32) {
     const uint32_t q = base + lane;
     uint32_t start = 0, len = 0;
-    if (q < ee) {
-      const uint32_t r = rcol[q];
-      start = prb_rp[r];
-      len = prb_rp[r + 1] - start;
-    }
+    if (q < ee) segs.get(q, start, len);
     uint32_t incl = len;
 #pragma unroll
     for (uint32_t d = 1; d < 32; d <<= 1) {
@@ -114,13 +139,29 @@ __device__ __forceinline__ uint32_t probe_entries(const uint32_t* __restrict__ r
         if (sstart[owner + step] <= pbeg) owner += step;
       uint32_t nb = sstart[owner + 1];
       uint32_t bs = sbase[owner];
-      for (uint32_t p = pbeg; p < pend; p++) {
+      uint32_t p = pbeg;
+      // four independent loads in flight per lane
+      for (; p + 4 <= pend; p += 4) {
+        uint32_t x[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          while (p + k >= nb) {
+            owner++;
+            nb = sstart[owner + 1];
+            bs = sbase[owner];
+          }
+          x[k] = __ldg(prb_col + bs + p + k);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) hits += member<KIND>(bm, pv, x[k]);
+      }
+      for (; p < pend; p++) {
         while (p >= nb) {
           owner++;
           nb = sstart[owner + 1];
           bs = sbase[owner];
         }
-        hits += member<KIND>(bm, pv, prb_col[bs + p]);
+        hits += member<KIND>(bm, pv, __ldg(prb_col + bs + p));
       }
     }
     __syncwarp();
@@ -128,31 +169,81 @@ __device__ __forceinline__ uint32_t probe_entries(const uint32_t* __restrict__ r
   return hits;
 }
 
-// One work unit: entries [unit*K, min((unit+1)*K, nnz)) of the rows tile.
-template <uint32_t KIND>
-__device__ __forceinline__ unsigned long long run_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
-                                                       uint32_t* sstart, uint32_t* sbase, uint32_t lane) {
+// Build the pivot structure, probe entries [e, ee), restore the buffer to zero.
+template <uint32_t KIND, class Segs>
+__device__ __forceinline__ uint32_t pivot_pass(const uint32_t* __restrict__ prow, uint32_t pd, uint32_t base,
+                                               uint32_t words, const Segs& segs, uint32_t e, uint32_t ee,
+                                               const uint32_t* __restrict__ prb_col, uint32_t* bm, uint32_t* sstart,
+                                               uint32_t* sbase, uint32_t lane) {
+  if constexpr (KIND == kPivotBitmap) {
+    for (uint32_t i = lane; i < pd; i += 32) {
+      const uint32_t y = prow[i] - base;
+      atomicOr(&bm[y >> 5], 1u << (y & 31));
+    }
+  } else if constexpr (KIND == kPivotList) {
+    for (uint32_t i = lane; i < pd; i += 32) bm[i] = prow[i];
+  }
+  __syncwarp();
+  PivotView pv;
+  pv.row = prow;
+  pv.len = pd;
+  pv.base = base;
+  pv.span = words * 32;
+  pv.first = prow[0];
+  pv.last = prow[pd - 1];
+  const uint32_t hits = probe_entries<KIND>(segs, e, ee, prb_col, bm, sstart, sbase, pv, lane);
+  // the buffer is all-zero between pivots whatever kind used it last: the
+  // persistent queue hands one warp bitmap and list work in any order
+  __syncwarp();
+  if constexpr (KIND == kPivotBitmap) {
+    if (pd < words) {
+      for (uint32_t i = lane; i < pd; i += 32) bm[(prow[i] - base) >> 5] = 0;
+    } else {
+      for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
+    }
+  } else if constexpr (KIND == kPivotList) {
+    for (uint32_t i = lane; i < pd; i += 32) bm[i] = 0;
+  }
+  __syncwarp();
+  return hits;
+}
+
+// Row b of a tile holding entry e: the largest b with rp[b] <= e.
+__device__ __forceinline__ uint32_t row_of(const uint32_t* __restrict__ rp, uint32_t H, uint32_t e) {
+  uint32_t lo = 0, hi = H;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (rp[mid] <= e) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Next row after b with an entry at or after e (a warp-wide scan of row ends).
+__device__ __forceinline__ uint32_t next_row(const uint32_t* __restrict__ rp, uint32_t H, uint32_t b, uint32_t e,
+                                             uint32_t lane) {
+  b++;
+  while (true) {
+    const uint32_t idx = b + lane;
+    const uint32_t v = idx < H ? rp[idx + 1] : 0xffffffffu;
+    const uint32_t mask = __ballot_sync(FULL, v > e);
+    if (mask) return b + __ffs(mask) - 1;
+    b += 32;
+  }
+}
+
+// One per-task work unit: entries [unit*K, min((unit+1)*K, nnz)) of the rows tile.
+__device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
+                                                     uint32_t* sstart, uint32_t* sbase, uint32_t lane) {
   const uint32_t* __restrict__ r_rp = tk.rows.rp;
-  const uint32_t* __restrict__ r_col = tk.rows.col;
   const uint32_t* __restrict__ p_rp = tk.pivot.rp;
   const uint32_t* __restrict__ p_col = tk.pivot.col;
-  const uint32_t* __restrict__ q_rp = tk.probe.rp;
-  const uint32_t* __restrict__ q_col = tk.probe.col;
+  const TileSegs segs{tk.rows.col, tk.probe.rp};
   const uint32_t H = tk.rows.H;
   const uint64_t e0 = (uint64_t)unit * tk.unit_edges;
-  uint32_t e = (uint32_t)e0;
   const uint64_t e1w = e0 + tk.unit_edges;
+  uint32_t e = (uint32_t)e0;
   const uint32_t e1 = e1w < tk.rows.nnz ? (uint32_t)e1w : tk.rows.nnz;
-  // row b holding entry e: the largest b with rp[b] <= e
-  uint32_t b = 0;
-  {
-    uint32_t lo = 0, hi = H;
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (r_rp[mid] <= e) lo = mid; else hi = mid;
-    }
-    b = lo;
-  }
+  uint32_t b = row_of(r_rp, H, e);
   unsigned long long acc = 0;
   while (e < e1) {
     const uint32_t ee = min(r_rp[b + 1], e1);
@@ -160,45 +251,56 @@ __device__ __forceinline__ unsigned long long run_unit(const DevTask& tk, uint32
     const uint32_t pd = p_rp[b + 1] - ps;
     if (pd > 0) {
       const uint32_t* prow = p_col + ps;
-      if constexpr (KIND == kPivotBitmap) {
-        for (uint32_t i = lane; i < pd; i += 32) {
-          const uint32_t x = prow[i];
-          atomicOr(&bm[x >> 5], 1u << (x & 31));
-        }
-      } else if constexpr (KIND == kPivotList) {
-        for (uint32_t i = lane; i < pd; i += 32) bm[i] = prow[i];
+      switch (tk.kind) {
+        case kPivotBitmap:
+          acc += pivot_pass<kPivotBitmap>(prow, pd, 0, tk.words, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          break;
+        case kPivotList:
+          acc += pivot_pass<kPivotList>(prow, pd, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          break;
+        default:
+          acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
       }
-      __syncwarp();
-      PivotView pv;
-      pv.row = prow;
-      pv.len = pd;
-      pv.first = prow[0];
-      pv.last = prow[pd - 1];
-      acc += probe_entries<KIND>(r_col, e, ee, q_rp, q_col, bm, sstart, sbase, pv, lane);
-      if constexpr (KIND == kPivotBitmap) {
-        if (pd < tk.words) {
-          for (uint32_t i = lane; i < pd; i += 32) bm[prow[i] >> 5] = 0;
-        } else {
-          for (uint32_t i = lane; i < tk.words; i += 32) bm[i] = 0;
-        }
-      }
-      __syncwarp();
     }
     e = ee;
-    if (e < e1) {
-      // next row with an entry at or after e
-      b++;
-      while (true) {
-        const uint32_t idx = b + lane;
-        const uint32_t v = idx < H ? r_rp[idx + 1] : 0xffffffffu;
-        const uint32_t mask = __ballot_sync(FULL, v > e);
-        if (mask) {
-          b += __ffs(mask) - 1;
-          break;
-        }
-        b += 32;
-      }
+    if (e < e1) b = next_row(r_rp, H, b, e, lane);
+  }
+  return acc;
+}
+
+// One fused task-row unit: in-edges [unit*K, ...) of the reversed tile (j, i).
+__device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
+                                                      uint32_t* sstart, uint32_t* sbase, uint32_t lane,
+                                                      uint32_t bm_words) {
+  const uint32_t* __restrict__ r_rp = tk.rows.rp;
+  const uint32_t* __restrict__ gp = tk.g_indptr;
+  const uint32_t* __restrict__ gi = tk.g_indices;
+  const RecSegs segs{tk.rows.rec};
+  const uint32_t H = tk.rows.H;
+  const uint64_t e0 = (uint64_t)unit * tk.unit_edges;
+  const uint64_t e1w = e0 + tk.unit_edges;
+  uint32_t e = (uint32_t)e0;
+  const uint32_t e1 = e1w < tk.rows.nnz ? (uint32_t)e1w : tk.rows.nnz;
+  uint32_t b = row_of(r_rp, H, e);
+  unsigned long long acc = 0;
+  while (e < e1) {
+    const uint32_t ee = min(r_rp[b + 1], e1);
+    const uint32_t v = tk.pivot_base + b;
+    const uint32_t ps = gp[v];
+    const uint32_t pd = gp[v + 1] - ps;
+    if (pd > 0) {
+      const uint32_t* prow = gi + ps;
+      const uint32_t first = prow[0];
+      const uint32_t span_words = ((prow[pd - 1] - first) >> 5) + 1;
+      if (span_words <= bm_words)
+        acc += pivot_pass<kPivotBitmap>(prow, pd, first, span_words, segs, e, ee, gi, bm, sstart, sbase, lane);
+      else if (pd <= bm_words)
+        acc += pivot_pass<kPivotList>(prow, pd, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+      else
+        acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
     }
+    e = ee;
+    if (e < e1) b = next_row(r_rp, H, b, e, lane);
   }
   return acc;
 }
@@ -210,19 +312,17 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 }
 
 __device__ __forceinline__ unsigned long long dispatch_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
-                                                            uint32_t* sstart, uint32_t* sbase, uint32_t lane) {
-  switch (tk.kind) {
-    case kPivotBitmap: return run_unit<kPivotBitmap>(tk, unit, bm, sstart, sbase, lane);
-    case kPivotList: return run_unit<kPivotList>(tk, unit, bm, sstart, sbase, lane);
-    default: return run_unit<kPivotGlobal>(tk, unit, bm, sstart, sbase, lane);
-  }
+                                                            uint32_t* sstart, uint32_t* sbase, uint32_t lane,
+                                                            uint32_t bm_words) {
+  if (tk.kind == kFusedRow) return fused_unit(tk, unit, bm, sstart, sbase, lane, bm_words);
+  return task_unit(tk, unit, bm, sstart, sbase, lane);
 }
 
 // Persistent form: every warp claims units from one head until the queue is empty.
-__global__ void __launch_bounds__(256) k_count_queue(const DevTask* __restrict__ tasks,
-                                                     const uint32_t* __restrict__ prefix, uint32_t ntasks,
-                                                     uint32_t total_units, uint32_t* __restrict__ head,
-                                                     unsigned long long* __restrict__ outs, uint32_t bm_words) {
+__global__ void __launch_bounds__(256, 4) k_count_queue(const DevTask* __restrict__ tasks,
+                                                        const uint32_t* __restrict__ prefix, uint32_t ntasks,
+                                                        uint32_t total_units, uint32_t* __restrict__ head,
+                                                        unsigned long long* __restrict__ outs, uint32_t bm_words) {
   extern __shared__ __align__(16) uint32_t sh[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
@@ -241,14 +341,14 @@ __global__ void __launch_bounds__(256) k_count_queue(const DevTask* __restrict__
       if (prefix[mid] <= g) lo = mid; else hi = mid;
     }
     const DevTask& tk = tasks[lo];
-    const unsigned long long c = warp_sum(dispatch_unit(tk, g - prefix[lo], bm, sstart, sbase, lane));
+    const unsigned long long c = warp_sum(dispatch_unit(tk, g - prefix[lo], bm, sstart, sbase, lane, bm_words));
     if (lane == 0 && c) atomicAdd(&outs[tk.slot], c);
   }
 }
 
 // Plain form: one task per launch; warps stride over the task's units.
-__global__ void __launch_bounds__(256) k_count_task(const DevTask* __restrict__ task, uint32_t units,
-                                                    unsigned long long* __restrict__ outs, uint32_t bm_words) {
+__global__ void __launch_bounds__(256, 4) k_count_task(const DevTask* __restrict__ task, uint32_t units,
+                                                       unsigned long long* __restrict__ outs, uint32_t bm_words) {
   extern __shared__ __align__(16) uint32_t sh[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
@@ -260,7 +360,7 @@ __global__ void __launch_bounds__(256) k_count_task(const DevTask* __restrict__ 
   const uint32_t wpb = blockDim.x >> 5;
   unsigned long long acc = 0;
   for (uint32_t u = blockIdx.x * wpb + warp; u < units; u += gridDim.x * wpb)
-    acc += dispatch_unit(tk, u, bm, sstart, sbase, lane);
+    acc += dispatch_unit(tk, u, bm, sstart, sbase, lane, bm_words);
   acc = warp_sum(acc);
   if (lane == 0 && acc) atomicAdd(&outs[tk.slot], acc);
 }
@@ -270,7 +370,7 @@ size_t smem_bytes(uint32_t bm_words, uint32_t warps) {
 }
 
 uint32_t norm_bm_words(uint32_t w) {
-  if (w == 0) w = 2048;
+  if (w == 0) w = 1024;
   w = (w + 3) & ~3u;
   return std::max<uint32_t>(w, 32);
 }
@@ -289,18 +389,52 @@ int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o) {
   return BBTC_OK;
 }
 
+// Average out-row length of row part i over its tiles (for unit sizing).
+static double part_row_len(const bbtc_graph* g, uint32_t i) {
+  uint64_t z = 0;
+  uint32_t rows = 1;
+  for (uint32_t k = 0; k < g->P; k++) {
+    z += g->fwd.nnz[i * g->P + k];
+    rows = std::max(rows, g->fwd.nerows[i * g->P + k]);
+  }
+  return (double)z / rows;
+}
+
 // Build the device task array for a request.  A single graph keeps the
 // caller's task order (its border split); several graphs are merged into one
-// queue ordered by estimated probe work, heaviest first.
+// queue ordered by estimated probe work, heaviest first.  With `fused`, every
+// graph's full task list runs as task rows (i, j).
 static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<std::vector<bbtc_task>>& tasks,
-                     const bbtc_opts& o, Plan* plan) {
+                     const bbtc_opts& o, bool fused, Plan* plan) {
   const uint32_t bmw = norm_bm_words(o.bitmap_words);
   const uint32_t unit_work = o.unit_work ? o.unit_work : 8192;
   std::vector<DevTask> list;
   std::vector<double> cost;
+  auto add = [&](DevTask d, double avg_probe) {
+    uint32_t K = (uint32_t)std::min(16384.0, std::max(32.0, unit_work / std::max(1.0, avg_probe)));
+    K = (K + 31) & ~31u;
+    d.unit_edges = K;
+    list.push_back(d);
+    cost.push_back((double)d.rows.nnz * std::max(1.0, avg_probe));
+  };
   for (size_t gi = 0; gi < graphs.size(); gi++) {
     const bbtc_graph* g = graphs[gi];
     const uint32_t P = g->P;
+    if (fused) {
+      for (uint32_t i = 0; i < P; i++)
+        for (uint32_t j = i; j < P; j++) {
+          if (!g->fwd.nnz[i * P + j]) continue;
+          DevTask d{};
+          d.rows = dev_tile(g->rev, g->cuts, j, i);
+          d.kind = kFusedRow;
+          d.slot = (uint32_t)gi;
+          d.g_indptr = g->d_indptr;
+          d.g_indices = g->d_indices;
+          d.pivot_base = g->cuts[j];
+          add(d, 0.5 * part_row_len(g, i));
+        }
+      continue;
+    }
     for (const bbtc_task& t : tasks[gi]) {
       if (t.ab >= P * P || t.bc >= P * P || t.ac >= P * P)
         return fail(BBTC_ERR_ARG, "task names a tile outside the P x P grid");
@@ -319,28 +453,22 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
         d.pivot = dev_tile(g->fwd, g->cuts, j, k);
         d.probe = dev_tile(g->fwd, g->cuts, i, k);
       }
-      const uint32_t W = d.pivot.W;
-      d.words = (W + 31) / 32;
+      d.words = (d.pivot.W + 31) / 32;
       const bool fits_bitmap = d.words <= bmw;
       const bool fits_list = d.pivot.maxdeg <= bmw;
       if (!u_centric && o.kernel != BBTC_KERNEL_SEARCH && fits_bitmap)
         d.kind = kPivotBitmap;
       else
         d.kind = fits_list ? kPivotList : kPivotGlobal;
+      d.slot = (uint32_t)gi;
       const uint32_t probe_tile = u_centric ? j * P + k : i * P + k;
       const uint32_t probe_rows = std::max<uint32_t>(1, g->fwd.nerows[probe_tile]);
-      const double avg = std::max(1.0, (double)d.probe.nnz / probe_rows);
-      uint32_t K = (uint32_t)std::min(16384.0, std::max(32.0, unit_work / avg));
-      K = (K + 31) & ~31u;
-      d.unit_edges = K;
-      d.slot = (uint32_t)gi;
-      list.push_back(d);
-      cost.push_back((double)d.rows.nnz * avg);
+      add(d, (double)d.probe.nnz / probe_rows);
     }
   }
   std::vector<uint32_t> order(list.size());
   for (uint32_t q = 0; q < order.size(); q++) order[q] = q;
-  if (graphs.size() > 1)
+  if (graphs.size() > 1 || fused)
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
   plan->tasks.clear();
   plan->prefix.assign(1, 0);
@@ -399,13 +527,13 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
 }
 
 int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
-                  const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o, uint64_t* d_outs,
-                  Plan* plan, bool reuse) {
+                  const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o, bool fused,
+                  uint64_t* d_outs, Plan* plan, bool reuse) {
   cudaStream_t s = ctx->stream;
   BBTC_TRY(kernel_smem_optin(ctx, o));
   if (!reuse) {
     plan->release();
-    BBTC_TRY(make_plan(graphs, tasks, o, plan));
+    BBTC_TRY(make_plan(graphs, tasks, o, fused, plan));
     const size_t nt = plan->tasks.size();
     if (nt) {
       if (cudaMalloc(&plan->d_tasks, nt * sizeof(DevTask)) != cudaSuccess ||

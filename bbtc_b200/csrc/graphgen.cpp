@@ -189,10 +189,17 @@ int gen_rmat(int scale, int ef, double a, double b, double c, uint64_t seed, Csr
   return clean_and_orient(n, src.data(), dst.data(), m, out);
 }
 
-// Σ_{i=0}^{n-1} (i + i0)^(-alpha), by the midpoint integral (used only to pick i0)
+// Σ_{i=0}^{n-1} (i + i0)^(-alpha): the first 1024 terms exactly, the tail by
+// the midpoint integral (used only to pick i0)
 double approx_power_sum(double n, double i0, double alpha) {
-  const double lo = i0 - 0.5, hi = n + i0 - 0.5;
-  return (std::pow(hi, 1.0 - alpha) - std::pow(lo, 1.0 - alpha)) / (1.0 - alpha);
+  const double head = std::min(n, 1024.0);
+  double s = 0;
+  for (double i = 0; i < head; i += 1) s += std::pow(i + i0, -alpha);
+  if (n > head) {
+    const double lo = head + i0 - 0.5, hi = n + i0 - 0.5;
+    s += (std::pow(hi, 1.0 - alpha) - std::pow(lo, 1.0 - alpha)) / (1.0 - alpha);
+  }
+  return s;
 }
 
 int gen_chung_lu(uint32_t n, double gamma, double mean_deg, double max_deg, uint64_t seed, Csr* out) {
@@ -200,8 +207,8 @@ int gen_chung_lu(uint32_t n, double gamma, double mean_deg, double max_deg, uint
   const double alpha = 1.0 / (gamma - 1.0);
   // pick i0 so that max/mean = n * i0^-alpha / Σ (i+i0)^-alpha
   const double target = max_deg / mean_deg;
-  double lo = 1e-6, hi = (double)n;
-  for (int it = 0; it < 200; it++) {
+  double lo = 1e-3, hi = (double)n;
+  for (int it = 0; it < 100; it++) {
     const double mid = std::sqrt(lo * hi);
     const double ratio = n * std::pow(mid, -alpha) / approx_power_sum(n, mid, alpha);
     if (ratio > target) lo = mid; else hi = mid;  // ratio falls as i0 grows
@@ -372,6 +379,20 @@ int bbtcg_rgg(uint32_t n, double radius, uint64_t seed, void** handle) {
 int bbtcg_from_pairs(uint32_t n, const uint32_t* src, const uint32_t* dst, uint64_t m, void** handle) {
   if (m && (!src || !dst)) return -1;
   return make(handle, [&](Csr* g) { return clean_and_orient(n, src, dst, m, g); });
+}
+
+// Wrap an already oriented CSR (copied, not cleaned: the counting library
+// checks the input contract on upload).
+int bbtcg_from_csr(uint32_t n, const uint32_t* indptr, const uint32_t* indices, uint64_t m, void** handle) {
+  if (!indptr || (m && !indices)) return -1;
+  if (m >= (1ull << 32)) return -3;
+  return make(handle, [&](Csr* g) {
+    g->n = n;
+    g->indptr.assign(indptr, indptr + (size_t)n + 1);
+    g->indices.assign(indices, indices + m);
+    g->m_raw = m;
+    return 0;
+  });
 }
 
 int bbtcg_info(void* handle, uint32_t* n, uint64_t* m, uint64_t* m_raw) {

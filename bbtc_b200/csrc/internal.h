@@ -39,6 +39,7 @@ constexpr uint64_t kNoSegment = ~0ull;
 struct DevTile {
   const uint32_t* rp;
   const uint32_t* col;
+  const uint2* rec;  // reversed tiles: (e + 1, end of row u) of each entry's forward edge e = (u, v)
   uint32_t H, W, nnz, maxdeg;
 };
 
@@ -47,6 +48,7 @@ enum TaskKind : uint32_t {
   kPivotBitmap = 0,  // pivot row -> shared bitmap of the column part, probes test bits
   kPivotList = 1,    // pivot row -> sorted shared list, probes binary-search it
   kPivotGlobal = 2,  // pivot row too long for shared memory: binary search in global memory
+  kFusedRow = 3,     // task row (i, j): all tasks (i, j, k >= j) in one pass, structure chosen per pivot
 };
 
 // One queued task: `rows` is the tile whose rows are the pivot vertices and
@@ -59,6 +61,9 @@ struct DevTask {
   DevTile rows;
   DevTile pivot;
   DevTile probe;
+  const uint32_t* g_indptr;   // fused task rows: the resident oriented CSR
+  const uint32_t* g_indices;
+  uint32_t pivot_base;        // fused: first vertex id of part j
   uint32_t kind;
   uint32_t unit_edges;  // entries of `rows` per work unit
   uint32_t slot;        // output counter index
@@ -72,8 +77,10 @@ struct BlockTiles {
   std::vector<uint64_t> rp_off, col_off;      // element offsets, kNoSegment when empty
   uint32_t* d_rp = nullptr;                    // row-pointer pool
   uint32_t* d_col = nullptr;                   // column pool
+  void* d_rec = nullptr;                       // reversed tiles: forward-edge records (uint2), col-aligned
   size_t rp_len = 0, col_len = 0;
-  void release();
+  cudaStream_t stream = nullptr;
+  void release(cudaStream_t s);
 };
 
 struct Plan {
@@ -103,6 +110,8 @@ struct bbtc_graph {
   uint32_t n = 0, P = 0;
   uint64_t m = 0;
   std::vector<uint32_t> cuts;
+  uint32_t* d_indptr = nullptr;   // resident oriented CSR (global ids)
+  uint32_t* d_indices = nullptr;
   bbtc::BlockTiles fwd, rev;
   uint64_t* d_count = nullptr;  // result slot
   uint64_t device_bytes = 0;
@@ -114,12 +123,14 @@ struct bbtc_graph {
 namespace bbtc {
 
 // layout.cu
-int build_layout(bbtc_graph* g, const uint32_t* d_indptr, const uint32_t* d_indices);
+// indptr / indices are host memory when `host`, else device memory of the
+// context's device; the graph keeps its own device copy either way.
+int build_layout(bbtc_graph* g, const uint32_t* indptr, const uint32_t* indices, bool host);
 DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_t x, uint32_t y);
 
 // count.cu
 int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
-                  const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o,
+                  const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o, bool fused,
                   uint64_t* d_outs, Plan* plan, bool reuse);
 int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o);
 

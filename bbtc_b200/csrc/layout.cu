@@ -8,14 +8,20 @@
 // (src/triangle_counting/bb_tc_helper.cpp:75-110).  Here the whole layout is
 // built on the device once and stays resident:
 //
+//   * the oriented CSR itself (global ids), which the fused task rows probe;
 //   * forward tiles (x, y): rows of part x, tile-local columns of part y --
-//     the reference's tiles, used as ab / bc / ac;
+//     the reference's tiles, used as ab / bc / ac by the per-task kernels;
 //   * reversed tiles (y, x): the same edges grouped by their column vertex --
-//     the CSC of forward tile (x, y), which the pivot-row kernels walk.
+//     the CSC of forward tile (x, y) -- with, beside each entry, the record
+//     (e + 1, end of row u) of its forward edge e = (u, v): the ids of N+(u)
+//     that follow v, which is what a fused task row streams per entry.
 //
-// Each non-empty tile owns a row-pointer segment of H+1 tile-local offsets
-// (first entry 0) and a column segment of nnz ids; both start on a 16-byte
-// boundary (multiples of 4 words) inside two pools.  Empty tiles own nothing.
+// Every tile owns a row-pointer segment of H+1 tile-local offsets (first
+// entry 0) in one pool, laid out like the reference's rows_ array (P segments
+// per row part); column segments hold only the non-empty tiles.  Segments
+// start on 16-byte boundaries.  All passes are edge-parallel: each edge finds
+// its tile by bisection of the cut vector and the first edge of every (row,
+// tile) run writes the run length, so no thread walks a whole row.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -27,6 +33,8 @@ namespace bbtc {
 
 namespace {
 
+constexpr uint32_t FULLMASK = 0xffffffffu;
+
 __device__ __forceinline__ uint32_t part_of(const uint32_t* cuts, uint32_t P, uint32_t u) {
   // largest x in [0, P) with cuts[x] <= u (skips empty parts); needs u < cuts[P]
   uint32_t lo = 0, hi = P;
@@ -37,135 +45,176 @@ __device__ __forceinline__ uint32_t part_of(const uint32_t* cuts, uint32_t P, ui
   return lo;
 }
 
+// first position p in [lo, hi) with a[p] >= x
+__device__ __forceinline__ uint32_t lower_bound_range(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
+                                                      uint32_t x) {
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (a[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
 // Input contract check: monotone row pointers, strictly increasing rows, ids < n.
-__global__ void k_validate(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
-                           uint32_t n, uint64_t m, uint32_t* __restrict__ bad) {
+__global__ void k_validate_rows(const uint32_t* __restrict__ indptr, uint32_t n, uint64_t m,
+                                uint32_t* __restrict__ bad) {
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
     if (u == 0 && indptr[0] != 0) atomicOr(bad, 1u);
     if (u == n - 1 && (uint64_t)indptr[n] != m) atomicOr(bad, 2u);
+    if (indptr[u + 1] < indptr[u] || (uint64_t)indptr[u + 1] > m) atomicOr(bad, 4u);
+  }
+}
+
+// Needs valid row pointers: expands the row id of every edge and checks ids.
+__global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+                               uint32_t n, uint32_t* __restrict__ rows, uint32_t* __restrict__ bad) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < n; u += nwarps) {
     const uint32_t a = indptr[u], b = indptr[u + 1];
-    if (b < a || (uint64_t)b > m) {
-      atomicOr(bad, 4u);
-      continue;
-    }
-    int64_t prev = -1;
-    for (uint32_t e = a; e < b; e++) {
+    for (uint32_t e = a + lane; e < b; e += 32) {
+      rows[e] = u;
       const uint32_t c = indices[e];
-      if (c >= n) { atomicOr(bad, 8u); break; }
-      if ((int64_t)c <= prev) { atomicOr(bad, 16u); break; }
-      prev = c;
+      if (c >= n) atomicOr(bad, 8u);
+      if (e > a && indices[e - 1] >= c) atomicOr(bad, 16u);
     }
   }
 }
 
-// Walk row u's entries as runs of one column part each; calls f(y, first, count).
-template <class F>
-__device__ __forceinline__ void for_each_run(const uint32_t* __restrict__ indices, uint32_t a, uint32_t b,
-                                             const uint32_t* cuts, F&& f) {
-  uint32_t y = 0;
-  uint32_t e = a;
-  while (e < b) {
-    const uint32_t c = indices[e];
-    while (c >= cuts[y + 1]) y++;
-    const uint32_t hi = cuts[y + 1];
-    uint32_t e2 = e + 1;
-    while (e2 < b && indices[e2] < hi) e2++;
-    f(y, e, e2 - e);
-    e = e2;
-  }
-}
-
-// Per-tile nnz, longest row and non-empty row count (CTA histograms in shared memory).
-__global__ void k_tile_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
-                             uint32_t n, const uint32_t* __restrict__ cuts_g, uint32_t P,
-                             uint32_t* __restrict__ nnz, uint32_t* __restrict__ maxdeg,
-                             uint32_t* __restrict__ nerows) {
-  extern __shared__ uint32_t sh[];
-  const uint32_t T = P * P;
-  uint32_t* h_nnz = sh;
-  uint32_t* h_max = sh + T;
-  uint32_t* h_ne = sh + 2 * T;
-  uint32_t* cuts = sh + 3 * T;
-  for (uint32_t t = threadIdx.x; t < 3 * T; t += blockDim.x) sh[t] = 0;
-  for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
-  __syncthreads();
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
-    const uint32_t x = part_of(cuts, P, u);
-    const uint32_t a = indptr[u], b = indptr[u + 1];
-    for_each_run(indices, a, b, cuts, [&](uint32_t y, uint32_t, uint32_t cnt) {
-      const uint32_t t = x * P + y;
-      atomicAdd(&h_nnz[t], cnt);
-      atomicMax(&h_max[t], cnt);
-      atomicAdd(&h_ne[t], 1u);
-    });
-  }
-  __syncthreads();
-  for (uint32_t t = threadIdx.x; t < T; t += blockDim.x) {
-    if (h_nnz[t]) {
-      atomicAdd(&nnz[t], h_nnz[t]);
-      atomicMax(&maxdeg[t], h_max[t]);
-      atomicAdd(&nerows[t], h_ne[t]);
-    }
-  }
-}
-
-// rp_pool[rp_off[t] + r + 1] = length of row r in tile t.
-__global__ void k_row_counts(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
-                             uint32_t n, const uint32_t* __restrict__ cuts_g, uint32_t P,
-                             const uint64_t* __restrict__ rp_off, uint32_t* __restrict__ pool) {
+// Run lengths: the first edge of each (row, tile) run writes the length into
+// slot (rp_off[tile] + local row + 1) of the counts buffer.
+__global__ void k_entry_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+                              const uint32_t* __restrict__ rows, uint64_t m, const uint32_t* __restrict__ cuts_g,
+                              uint32_t P, const uint64_t* __restrict__ rp_off, uint32_t* __restrict__ counts) {
   __shared__ uint32_t cuts[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
   __syncthreads();
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
+    const uint32_t u = rows[e];
+    const uint32_t c = indices[e];
+    const uint32_t y = part_of(cuts, P, c);
+    const uint32_t a = indptr[u];
+    if (e > a && indices[e - 1] >= cuts[y]) continue;  // not the first edge of its run
+    const uint32_t end = lower_bound_range(indices, (uint32_t)e, indptr[u + 1], cuts[y + 1]);
     const uint32_t x = part_of(cuts, P, u);
-    const uint32_t r = u - cuts[x];
-    for_each_run(indices, indptr[u], indptr[u + 1], cuts, [&](uint32_t y, uint32_t, uint32_t cnt) {
-      pool[rp_off[x * P + y] + r + 1] = cnt;
-    });
+    counts[rp_off[x * P + y] + (u - cuts[x]) + 1] = end - (uint32_t)e;
   }
 }
 
-// After an inclusive scan over the whole pool, make each segment tile-local.
-__global__ void k_localize(uint32_t* __restrict__ pool, uint64_t len, const uint64_t* __restrict__ seg_start,
-                           const uint32_t* __restrict__ seg_base, uint32_t nseg) {
+// base[t] = value of the scanned pool at tile t's first slot (sum of all earlier counts).
+__global__ void k_tile_base(const uint32_t* __restrict__ rp, const uint64_t* __restrict__ rp_off, uint32_t T,
+                            uint32_t* __restrict__ base) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
+    base[t] = rp[rp_off[t]];
+}
+
+// Subtract each tile's base from its slots: row pointers become tile-local.
+__global__ void k_localize(uint32_t* __restrict__ rp, uint32_t P, const uint64_t* __restrict__ part_off,
+                           const uint32_t* __restrict__ base, uint64_t len) {
+  __shared__ uint64_t poff[kMaxParts + 1];
+  for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) poff[t] = part_off[t];
+  __syncthreads();
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < len; s += stride) {
-    uint32_t lo = 0, hi = nseg;  // last q with seg_start[q] <= s
+    uint32_t lo = 0, hi = P;  // row part x: last x with part_off[x] <= s
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
-      if (seg_start[mid] <= s) lo = mid; else hi = mid;
+      if (poff[mid] <= s) lo = mid; else hi = mid;
     }
-    pool[s] -= seg_base[lo];
+    const uint64_t A = (poff[lo + 1] - poff[lo]) / P;  // slots per tile of this row part
+    const uint32_t y = (uint32_t)((s - poff[lo]) / A);
+    rp[s] -= base[lo * P + y];
   }
 }
 
-__global__ void k_scatter(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
-                          uint32_t n, const uint32_t* __restrict__ cuts_g, uint32_t P,
-                          const uint64_t* __restrict__ rp_off, const uint64_t* __restrict__ col_off,
-                          const uint32_t* __restrict__ rp_pool, uint32_t* __restrict__ col_pool) {
+// Longest row and non-empty rows per tile, from the local row pointers;
+// lanes of one tile are combined before the atomics.
+__global__ void k_rowstats(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cuts_g, uint32_t P,
+                           const uint64_t* __restrict__ part_off, uint64_t len, uint32_t* __restrict__ maxdeg,
+                           uint32_t* __restrict__ nerows) {
+  __shared__ uint32_t cuts[kMaxParts + 1];
+  __shared__ uint64_t poff[kMaxParts + 1];
+  for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) {
+    cuts[t] = cuts_g[t];
+    poff[t] = part_off[t];
+  }
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t start = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t iters = (len + stride - 1) / stride;  // the same for every lane of a warp
+  for (uint64_t it = 0; it < iters; it++) {
+    const uint64_t s = start + it * stride;
+    uint32_t tile = 0xffffffffu, rowlen = 0;
+    if (s < len) {
+      uint32_t lo = 0, hi = P;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (poff[mid] <= s) lo = mid; else hi = mid;
+      }
+      const uint64_t A = (poff[lo + 1] - poff[lo]) / P;
+      const uint32_t y = (uint32_t)((s - poff[lo]) / A);
+      const uint32_t r = (uint32_t)(s - poff[lo] - (uint64_t)y * A);
+      if (r < cuts[lo + 1] - cuts[lo]) {
+        rowlen = rp[s + 1] - rp[s];
+        tile = lo * P + y;
+      }
+    }
+    const uint32_t grp = __match_any_sync(FULLMASK, tile);
+    const uint32_t mx = __reduce_max_sync(grp, rowlen);
+    const uint32_t ne = __popc(grp & __ballot_sync(FULLMASK, rowlen != 0));
+    if (tile != 0xffffffffu && lane == (uint32_t)(__ffs(grp) - 1)) {
+      if (ne) atomicAdd(&nerows[tile], ne);
+      if (mx) atomicMax(&maxdeg[tile], mx);
+    }
+  }
+}
+
+// nnz per tile and 16-byte aligned column offsets of the non-empty tiles (one block).
+__global__ void k_tile_offsets(const uint32_t* __restrict__ rp, const uint64_t* __restrict__ rp_off,
+                               const uint32_t* __restrict__ cuts, uint32_t P, uint32_t* __restrict__ nnz,
+                               uint64_t* __restrict__ col_off) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint64_t cur = 0;
+  for (uint32_t t = 0; t < P * P; t++) {
+    const uint32_t x = t / P;
+    const uint32_t z = rp[rp_off[t] + (cuts[x + 1] - cuts[x])];
+    nnz[t] = z;
+    col_off[t] = z ? cur : kNoSegment;
+    cur += ((uint64_t)z + 3) & ~3ull;
+  }
+}
+
+// Scatter tile-local column ids (and, for the reversed graph, the records of
+// the forward edges) into the column pool.
+__global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+                                const uint32_t* __restrict__ rows, uint64_t m, const uint32_t* __restrict__ cuts_g,
+                                uint32_t P, const uint64_t* __restrict__ rp_off, const uint64_t* __restrict__ col_off,
+                                const uint32_t* __restrict__ rp, uint32_t* __restrict__ col,
+                                const uint32_t* __restrict__ eids, const uint32_t* __restrict__ fwd_indptr,
+                                uint2* __restrict__ rec) {
   __shared__ uint32_t cuts[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
   __syncthreads();
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
+    const uint32_t u = rows[e];
+    const uint32_t c = indices[e];
+    const uint32_t y = part_of(cuts, P, c);
     const uint32_t x = part_of(cuts, P, u);
-    const uint32_t r = u - cuts[x];
-    for_each_run(indices, indptr[u], indptr[u + 1], cuts, [&](uint32_t y, uint32_t first, uint32_t cnt) {
-      const uint32_t t = x * P + y;
-      uint32_t* dst = col_pool + col_off[t] + rp_pool[rp_off[t] + r];
-      const uint32_t base = cuts[y];
-      for (uint32_t q = 0; q < cnt; q++) dst[q] = indices[first + q] - base;
-    });
+    const uint32_t t = x * P + y;
+    const uint32_t a = indptr[u];
+    const uint32_t run = lower_bound_range(indices, a, (uint32_t)e, cuts[y]);
+    const uint64_t pos = col_off[t] + rp[rp_off[t] + (u - cuts[x])] + ((uint32_t)e - run);
+    col[pos] = c - cuts[y];
+    if (rec) {
+      const uint32_t fe = eids[e];  // forward edge (c -> u) of this reversed entry
+      rec[pos] = make_uint2(fe + 1, fwd_indptr[c + 1]);
+    }
   }
-}
-
-__global__ void k_expand_rows(const uint32_t* __restrict__ indptr, uint32_t n, uint32_t* __restrict__ rows) {
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride)
-    for (uint32_t e = indptr[u]; e < indptr[u + 1]; e++) rows[e] = u;
 }
 
 // rev_indptr[v] = first position of key v in the sorted keys (v in [0, n]).
@@ -182,19 +231,34 @@ __global__ void k_rev_indptr(const uint32_t* __restrict__ keys, uint64_t m, uint
   }
 }
 
+__global__ void k_iota(uint32_t* __restrict__ a, uint64_t m) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) a[e] = (uint32_t)e;
+}
+
+// rev_cols[q] = row (source) of the forward edge eids[q]
+__global__ void k_gather(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, uint64_t m,
+                         uint32_t* __restrict__ dst) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) dst[e] = src[idx[e]];
+}
+
 inline uint64_t align4(uint64_t x) { return (x + 3) & ~3ull; }
 
+// Stream-ordered device buffer (freed on the context stream).
 struct DevBuf {
   void* p = nullptr;
+  cudaStream_t s = nullptr;
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
   }
   template <class T>
   T* as() { return static_cast<T*>(p); }
 };
 
-int dalloc(DevBuf& b, size_t bytes) {
-  cudaError_t e = cudaMalloc(&b.p, std::max<size_t>(bytes, 16));
+int dalloc(DevBuf& b, size_t bytes, cudaStream_t s) {
+  b.s = s;
+  cudaError_t e = cudaMallocAsync(&b.p, std::max<size_t>(bytes, 16), s);
   if (e != cudaSuccess) {
     cudaGetLastError();
     b.p = nullptr;
@@ -204,108 +268,101 @@ int dalloc(DevBuf& b, size_t bytes) {
   return BBTC_OK;
 }
 
-// Build one block CSR (forward or reversed) from a CSR in device memory.
-int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const uint32_t* d_indices, uint32_t n,
-                uint64_t m, const std::vector<uint32_t>& cuts, const uint32_t* d_cuts, int grid) {
+// Build one block CSR (forward or reversed) from a CSR in device memory whose
+// per-edge row ids are `rows`.  With `eids` the reversed build also writes the
+// forward-edge records.  The tile statistics land in `st` (device, 4*P*P words)
+// and are copied to the host by the caller.
+int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const uint32_t* d_indices,
+                const uint32_t* d_rows, uint32_t n, uint64_t m, const std::vector<uint32_t>& cuts,
+                const uint32_t* d_cuts, const uint32_t* eids, const uint32_t* fwd_indptr, uint32_t* d_stats,
+                uint64_t* d_coloff, int grid) {
   const uint32_t P = (uint32_t)cuts.size() - 1;
   const uint32_t T = P * P;
   cudaStream_t s = ctx->stream;
   bt.P = P;
-  bt.nnz.assign(T, 0);
-  bt.maxdeg.assign(T, 0);
-  bt.nerows.assign(T, 0);
-  bt.rp_off.assign(T, kNoSegment);
-  bt.col_off.assign(T, kNoSegment);
-
-  DevBuf stats;
-  BBTC_TRY(dalloc(stats, 3 * T * sizeof(uint32_t)));
-  BBTC_CUDA(cudaMemsetAsync(stats.p, 0, 3 * T * sizeof(uint32_t), s));
-  if (n > 0) {
-    const size_t sm = (3 * T + P + 1) * sizeof(uint32_t);
-    if (sm > 48 * 1024)
-      BBTC_CUDA(cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_tile_count<<<grid, 256, sm, s>>>(d_indptr, d_indices, n, d_cuts, P, stats.as<uint32_t>(),
-                                       stats.as<uint32_t>() + T, stats.as<uint32_t>() + 2 * T);
-    BBTC_CUDA(cudaGetLastError());
+  bt.rp_off.assign(T, 0);
+  std::vector<uint64_t> part_off(P + 1, 0);
+  uint64_t cur = 0;
+  for (uint32_t x = 0; x < P; x++) {
+    part_off[x] = cur;
+    const uint64_t A = align4((uint64_t)cuts[x + 1] - cuts[x] + 1);
+    for (uint32_t y = 0; y < P; y++) bt.rp_off[x * P + y] = cur + y * A;
+    cur += A * P;
   }
-  std::vector<uint32_t> hst(3 * T);
-  BBTC_CUDA(cudaMemcpyAsync(hst.data(), stats.p, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  BBTC_CUDA(cudaStreamSynchronize(s));
-  std::copy(hst.begin(), hst.begin() + T, bt.nnz.begin());
-  std::copy(hst.begin() + T, hst.begin() + 2 * T, bt.maxdeg.begin());
-  std::copy(hst.begin() + 2 * T, hst.end(), bt.nerows.begin());
-
-  // segment offsets for the non-empty tiles, in row-major tile order
-  std::vector<uint64_t> seg_start;
-  std::vector<uint32_t> seg_base;
-  uint64_t rp_cur = 0, col_cur = 0, nnz_cur = 0;
-  for (uint32_t t = 0; t < T; t++) {
-    if (!bt.nnz[t]) continue;
-    const uint32_t x = t / P;
-    const uint64_t H = (uint64_t)cuts[x + 1] - cuts[x];
-    bt.rp_off[t] = rp_cur;
-    bt.col_off[t] = col_cur;
-    seg_start.push_back(rp_cur);
-    seg_base.push_back((uint32_t)nnz_cur);
-    rp_cur += align4(H + 1);
-    col_cur += align4(bt.nnz[t]);
-    nnz_cur += bt.nnz[t];
-  }
-  bt.rp_len = rp_cur + 4;  // a 16-byte tail keeps rounded-up bulk reads inside the pool
-  bt.col_len = col_cur + 4;
+  part_off[P] = cur;
+  bt.rp_len = cur + 4;  // a 16-byte tail keeps rounded-up reads inside the pool
+  bt.col_len = m + 4ull * T + 4;
   {
-    cudaError_t e1 = cudaMalloc(&bt.d_rp, bt.rp_len * sizeof(uint32_t));
-    cudaError_t e2 = cudaMalloc(&bt.d_col, bt.col_len * sizeof(uint32_t));
-    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+    cudaError_t e1 = cudaMallocAsync(&bt.d_rp, bt.rp_len * sizeof(uint32_t), s);
+    cudaError_t e2 = cudaMallocAsync(&bt.d_col, bt.col_len * sizeof(uint32_t), s);
+    cudaError_t e3 = eids ? cudaMallocAsync(&bt.d_rec, bt.col_len * sizeof(uint2), s) : cudaSuccess;
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
       cudaGetLastError();
-      bt.release();
+      bt.release(s);
       return fail(BBTC_ERR_NOMEM, "device allocation of the block-CSR pools failed");
     }
   }
-  if (seg_start.empty()) {
-    BBTC_CUDA(cudaMemsetAsync(bt.d_rp, 0, bt.rp_len * sizeof(uint32_t), s));
-    BBTC_CUDA(cudaMemsetAsync(bt.d_col, 0, bt.col_len * sizeof(uint32_t), s));
-    return BBTC_OK;
-  }
-  DevBuf offs, segs, counts;
-  BBTC_TRY(dalloc(offs, 2 * T * sizeof(uint64_t)));
-  BBTC_TRY(dalloc(segs, seg_start.size() * (sizeof(uint64_t) + sizeof(uint32_t))));
-  BBTC_TRY(dalloc(counts, bt.rp_len * sizeof(uint32_t)));
+  bt.stream = s;
+  DevBuf offs, counts, base;
+  BBTC_TRY(dalloc(offs, (T + P + 1) * sizeof(uint64_t), s));
+  BBTC_TRY(dalloc(counts, bt.rp_len * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(base, T * sizeof(uint32_t), s));
   uint64_t* d_rp_off = offs.as<uint64_t>();
-  uint64_t* d_col_off = d_rp_off + T;
-  uint64_t* d_seg_start = segs.as<uint64_t>();
-  uint32_t* d_seg_base = reinterpret_cast<uint32_t*>(d_seg_start + seg_start.size());
+  uint64_t* d_part_off = d_rp_off + T;
   BBTC_CUDA(cudaMemcpyAsync(d_rp_off, bt.rp_off.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-  BBTC_CUDA(cudaMemcpyAsync(d_col_off, bt.col_off.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-  BBTC_CUDA(cudaMemcpyAsync(d_seg_start, seg_start.data(), seg_start.size() * sizeof(uint64_t),
-                            cudaMemcpyHostToDevice, s));
-  BBTC_CUDA(cudaMemcpyAsync(d_seg_base, seg_base.data(), seg_base.size() * sizeof(uint32_t),
-                            cudaMemcpyHostToDevice, s));
+  BBTC_CUDA(cudaMemcpyAsync(d_part_off, part_off.data(), (P + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
   BBTC_CUDA(cudaMemsetAsync(counts.p, 0, bt.rp_len * sizeof(uint32_t), s));
   BBTC_CUDA(cudaMemsetAsync(bt.d_col, 0, bt.col_len * sizeof(uint32_t), s));
-  k_row_counts<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, d_cuts, P, d_rp_off, counts.as<uint32_t>());
-  BBTC_CUDA(cudaGetLastError());
+  BBTC_CUDA(cudaMemsetAsync(d_stats, 0, 4 * T * sizeof(uint32_t), s));
+  if (m > 0) {
+    k_entry_count<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, counts.as<uint32_t>());
+    BBTC_CUDA(cudaGetLastError());
+  }
   size_t tmp_bytes = 0;
-  BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, counts.as<uint32_t>(), bt.d_rp,
-                                          (int64_t)bt.rp_len, s));
+  BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, counts.as<uint32_t>(), bt.d_rp, (int64_t)bt.rp_len, s));
   DevBuf tmp;
-  BBTC_TRY(dalloc(tmp, tmp_bytes));
-  BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, counts.as<uint32_t>(), bt.d_rp,
-                                          (int64_t)bt.rp_len, s));
-  k_localize<<<grid, 256, 0, s>>>(bt.d_rp, bt.rp_len, d_seg_start, d_seg_base, (uint32_t)seg_start.size());
+  BBTC_TRY(dalloc(tmp, tmp_bytes, s));
+  BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, counts.as<uint32_t>(), bt.d_rp, (int64_t)bt.rp_len, s));
+  k_tile_base<<<(T + 255) / 256, 256, 0, s>>>(bt.d_rp, d_rp_off, T, base.as<uint32_t>());
   BBTC_CUDA(cudaGetLastError());
-  k_scatter<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, d_cuts, P, d_rp_off, d_col_off, bt.d_rp, bt.d_col);
+  uint32_t* st_nnz = d_stats;
+  uint32_t* st_max = d_stats + T;
+  uint32_t* st_ne = d_stats + 2 * T;
+  k_localize<<<grid, 256, 0, s>>>(bt.d_rp, P, d_part_off, base.as<uint32_t>(), part_off[P]);
   BBTC_CUDA(cudaGetLastError());
-  BBTC_CUDA(cudaStreamSynchronize(s));  // the temporaries above are freed on return
+  k_rowstats<<<grid, 256, 0, s>>>(bt.d_rp, d_cuts, P, d_part_off, part_off[P], st_max, st_ne);
+  BBTC_CUDA(cudaGetLastError());
+  k_tile_offsets<<<1, 32, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, st_nnz, d_coloff);
+  BBTC_CUDA(cudaGetLastError());
+  if (m > 0) {
+    k_entry_scatter<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
+                                         bt.d_col, eids, fwd_indptr, reinterpret_cast<uint2*>(bt.d_rec));
+    BBTC_CUDA(cudaGetLastError());
+  }
+  return BBTC_OK;
+}
+
+int fetch_stats(BlockTiles& bt, const uint32_t* d_stats, const uint64_t* d_coloff, cudaStream_t s) {
+  const uint32_t T = bt.P * bt.P;
+  std::vector<uint32_t> h(3 * T);
+  BBTC_CUDA(cudaMemcpyAsync(h.data(), d_stats, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  bt.col_off.assign(T, kNoSegment);
+  BBTC_CUDA(cudaMemcpyAsync(bt.col_off.data(), d_coloff, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  BBTC_CUDA(cudaStreamSynchronize(s));
+  bt.nnz.assign(h.begin(), h.begin() + T);
+  bt.maxdeg.assign(h.begin() + T, h.begin() + 2 * T);
+  bt.nerows.assign(h.begin() + 2 * T, h.end());
   return BBTC_OK;
 }
 
 }  // namespace
 
-void BlockTiles::release() {
-  if (d_rp) cudaFree(d_rp);
-  if (d_col) cudaFree(d_col);
+void BlockTiles::release(cudaStream_t s) {
+  if (d_rp) cudaFreeAsync(d_rp, s);
+  if (d_col) cudaFreeAsync(d_col, s);
+  if (d_rec) cudaFreeAsync(d_rec, s);
   d_rp = d_col = nullptr;
+  d_rec = nullptr;
 }
 
 DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_t x, uint32_t y) {
@@ -318,39 +375,70 @@ DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_
   if (d.nnz) {
     d.rp = t.d_rp + t.rp_off[id];
     d.col = t.d_col + t.col_off[id];
+    d.rec = t.d_rec ? reinterpret_cast<const uint2*>(t.d_rec) + t.col_off[id] : nullptr;
   } else {
     d.rp = d.col = nullptr;
+    d.rec = nullptr;
   }
   return d;
 }
 
-int build_layout(bbtc_graph* g, const uint32_t* d_indptr, const uint32_t* d_indices) {
+int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_indices, bool host) {
   bbtc_ctx* ctx = g->ctx;
   cudaStream_t s = ctx->stream;
   const uint32_t n = g->n;
   const uint64_t m = g->m;
+  const uint32_t P = g->P;
+  const uint32_t T = P * P;
   const int grid = ctx->sms * 8;
   cudaEvent_t ev0, ev1;
   BBTC_CUDA(cudaEventCreate(&ev0));
   BBTC_CUDA(cudaEventCreate(&ev1));
   struct EvGuard {
     cudaEvent_t a, b;
-    ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
   } evg{ev0, ev1};
   BBTC_CUDA(cudaEventRecord(ev0, s));
 
-  DevBuf d_cuts, bad;
-  BBTC_TRY(dalloc(d_cuts, g->cuts.size() * sizeof(uint32_t)));
-  BBTC_TRY(dalloc(bad, sizeof(uint32_t)));
+  // the graph keeps its own copy of the oriented CSR: the fused task rows probe it
+  {
+    cudaError_t e1 = cudaMallocAsync(&g->d_indptr, ((size_t)n + 1) * sizeof(uint32_t), s);
+    cudaError_t e2 = cudaMallocAsync(&g->d_indices, std::max<uint64_t>(m, 1) * sizeof(uint32_t) + 16, s);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+      cudaGetLastError();
+      return fail(BBTC_ERR_NOMEM, "device allocation of the CSR copy failed");
+    }
+    const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    BBTC_CUDA(cudaMemcpyAsync(g->d_indptr, in_indptr, ((size_t)n + 1) * sizeof(uint32_t), kind, s));
+    if (m) BBTC_CUDA(cudaMemcpyAsync(g->d_indices, in_indices, m * sizeof(uint32_t), kind, s));
+  }
+  const uint32_t* d_indptr = g->d_indptr;
+  const uint32_t* d_indices = g->d_indices;
+
+  DevBuf d_cuts, bad, rows, stats, coloff;
+  BBTC_TRY(dalloc(d_cuts, g->cuts.size() * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(bad, sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(rows, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(stats, 4 * T * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(coloff, T * sizeof(uint64_t), s));
   BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, g->cuts.data(), g->cuts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
-  if (n > 0) {
-    k_validate<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, bad.as<uint32_t>());
-    BBTC_CUDA(cudaGetLastError());
-  }
   uint32_t hbad = 0;
-  BBTC_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  BBTC_CUDA(cudaStreamSynchronize(s));
+  if (n > 0) {
+    k_validate_rows<<<grid, 256, 0, s>>>(d_indptr, n, m, bad.as<uint32_t>());
+    BBTC_CUDA(cudaGetLastError());
+    BBTC_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    BBTC_CUDA(cudaStreamSynchronize(s));
+    if (!hbad) {
+      k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, rows.as<uint32_t>(), bad.as<uint32_t>());
+      BBTC_CUDA(cudaGetLastError());
+      BBTC_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      BBTC_CUDA(cudaStreamSynchronize(s));
+    }
+  }
   if (hbad) {
     std::string why;
     if (hbad & 1) why += " indptr[0] != 0;";
@@ -361,37 +449,43 @@ int build_layout(bbtc_graph* g, const uint32_t* d_indptr, const uint32_t* d_indi
     return fail(BBTC_ERR_INPUT, "CSR breaks the input contract:" + why);
   }
 
-  BBTC_TRY(build_block(ctx, g->fwd, d_indptr, d_indices, n, m, g->cuts, d_cuts.as<uint32_t>(), grid));
+  BBTC_TRY(build_block(ctx, g->fwd, d_indptr, d_indices, rows.as<uint32_t>(), n, m, g->cuts, d_cuts.as<uint32_t>(),
+                       nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
+  BBTC_TRY(fetch_stats(g->fwd, stats.as<uint32_t>(), coloff.as<uint64_t>(), s));
 
-  // reversed graph: stable sort of (column, row) pairs by column keeps each in-list sorted
+  // reversed graph: a stable sort of (column, forward edge id) by column keeps
+  // every in-list ordered by source
   {
-    DevBuf keys_in, keys_out, vals_in, vals_out, rev_indptr;
-    BBTC_TRY(dalloc(keys_out, m * sizeof(uint32_t)));
-    BBTC_TRY(dalloc(vals_in, m * sizeof(uint32_t)));
-    BBTC_TRY(dalloc(vals_out, m * sizeof(uint32_t)));
-    BBTC_TRY(dalloc(rev_indptr, ((size_t)n + 1) * sizeof(uint32_t)));
+    DevBuf eids_in, keys_out, eids_out, rev_indptr, rev_cols;
+    BBTC_TRY(dalloc(keys_out, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+    BBTC_TRY(dalloc(eids_in, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+    BBTC_TRY(dalloc(eids_out, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+    BBTC_TRY(dalloc(rev_cols, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+    BBTC_TRY(dalloc(rev_indptr, ((size_t)n + 1) * sizeof(uint32_t), s));
     if (m > 0) {
-      k_expand_rows<<<grid, 256, 0, s>>>(d_indptr, n, vals_in.as<uint32_t>());
+      k_iota<<<grid, 256, 0, s>>>(eids_in.as<uint32_t>(), m);
       BBTC_CUDA(cudaGetLastError());
       int end_bit = 1;
       while (end_bit < 32 && (1ull << end_bit) < (uint64_t)n) end_bit++;
       size_t tmp_bytes = 0;
       BBTC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_indices, keys_out.as<uint32_t>(),
-                                                vals_in.as<uint32_t>(), vals_out.as<uint32_t>(), (int64_t)m,
-                                                0, end_bit, s));
+                                                eids_in.as<uint32_t>(), eids_out.as<uint32_t>(), (int64_t)m, 0,
+                                                end_bit, s));
       DevBuf tmp;
-      BBTC_TRY(dalloc(tmp, tmp_bytes));
+      BBTC_TRY(dalloc(tmp, tmp_bytes, s));
       BBTC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, d_indices, keys_out.as<uint32_t>(),
-                                                vals_in.as<uint32_t>(), vals_out.as<uint32_t>(), (int64_t)m,
-                                                0, end_bit, s));
-      k_rev_indptr<<<grid, 256, 0, s>>>(keys_out.as<uint32_t>(), m, n, rev_indptr.as<uint32_t>());
+                                                eids_in.as<uint32_t>(), eids_out.as<uint32_t>(), (int64_t)m, 0,
+                                                end_bit, s));
+      k_gather<<<grid, 256, 0, s>>>(rows.as<uint32_t>(), eids_out.as<uint32_t>(), m, rev_cols.as<uint32_t>());
       BBTC_CUDA(cudaGetLastError());
-      BBTC_CUDA(cudaStreamSynchronize(s));
-    } else {
-      BBTC_CUDA(cudaMemsetAsync(rev_indptr.p, 0, ((size_t)n + 1) * sizeof(uint32_t), s));
     }
-    BBTC_TRY(build_block(ctx, g->rev, rev_indptr.as<uint32_t>(), vals_out.as<uint32_t>(), n, m, g->cuts,
-                         d_cuts.as<uint32_t>(), grid));
+    k_rev_indptr<<<grid, 256, 0, s>>>(keys_out.as<uint32_t>(), m, n, rev_indptr.as<uint32_t>());
+    BBTC_CUDA(cudaGetLastError());
+    // reversed entries: row = column vertex v (keys), column = source u, record of forward edge (u, v)
+    BBTC_TRY(build_block(ctx, g->rev, rev_indptr.as<uint32_t>(), rev_cols.as<uint32_t>(), keys_out.as<uint32_t>(),
+                         n, m, g->cuts, d_cuts.as<uint32_t>(), eids_out.as<uint32_t>(), d_indptr,
+                         stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
+    BBTC_TRY(fetch_stats(g->rev, stats.as<uint32_t>(), coloff.as<uint64_t>(), s));
   }
   BBTC_CUDA(cudaEventRecord(ev1, s));
   BBTC_CUDA(cudaEventSynchronize(ev1));
@@ -399,7 +493,7 @@ int build_layout(bbtc_graph* g, const uint32_t* d_indptr, const uint32_t* d_indi
   BBTC_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   g->layout_ms = ms;
   g->device_bytes = (g->fwd.rp_len + g->fwd.col_len + g->rev.rp_len + g->rev.col_len) * sizeof(uint32_t) +
-                    sizeof(uint64_t);
+                    g->rev.col_len * sizeof(uint2) + ((uint64_t)n + 1 + m) * sizeof(uint32_t) + 64 * sizeof(uint64_t);
   return BBTC_OK;
 }
 

@@ -120,16 +120,20 @@ typedef enum bbtc_mode {
 } bbtc_mode;
 
 typedef enum bbtc_kernel {
-  BBTC_KERNEL_AUTO = 0,   /* per task: bitmap when the bc rows fit the bitmap, else search */
-  BBTC_KERNEL_BITMAP = 1, /* pivot row of bc as a shared-memory bitmap, probes from ac */
-  BBTC_KERNEL_SEARCH = 2, /* pivot row of bc as a sorted shared-memory list, binary-search probes */
-  BBTC_KERNEL_MERGE = 3   /* row of ab per warp, warp-cooperative merge/gallop of ac and bc rows */
+  BBTC_KERNEL_AUTO = 0,   /* persistent form over the whole task list: fused task rows; otherwise
+                             per task: bitmap when the part fits the shared bitmap, else search */
+  BBTC_KERNEL_BITMAP = 1, /* per task: pivot row of bc as a shared-memory bitmap, probes from ac */
+  BBTC_KERNEL_SEARCH = 2, /* per task: pivot row of bc as a sorted shared-memory list, bisection probes */
+  BBTC_KERNEL_MERGE = 3,  /* per task, the reference's row order: pivot = ac row of each ab row,
+                             the bc rows it meets are searched against it */
+  BBTC_KERNEL_FUSED = 4   /* task rows: the tasks (i, j, k >= j) sharing tile ab = (i, j) in one
+                             pass (needs the whole task list, tasks == NULL) */
 } bbtc_kernel;
 
 typedef struct bbtc_opts {
   int mode;                  /* bbtc_mode */
   int kernel;                /* bbtc_kernel */
-  uint32_t bitmap_words;     /* shared bitmap words per warp: 0 = default (2048) */
+  uint32_t bitmap_words;     /* shared bitmap / list words per warp: 0 = default (1024) */
   uint32_t warps_per_block;  /* 0 = default (8) */
   uint32_t unit_work;        /* target probes per work unit, 0 = default */
   uint32_t blocks_per_sm;    /* persistent grid = SMs x this, 0 = occupancy limit */

@@ -33,7 +33,7 @@ def test_version_and_defaults():
     assert core.lib().bbtc_version() >= 10000
     o = core.options()
     assert o.mode == core.MODE_PERSISTENT and o.kernel == core.KERNEL_AUTO
-    assert o.bitmap_words == 2048 and o.warps_per_block == 8 and o.use_cuda_graph == 1
+    assert o.bitmap_words == 1024 and o.warps_per_block == 8 and o.use_cuda_graph == 1
 
 
 def test_task_list_matches_reference_enumeration():

@@ -12,7 +12,7 @@ from bbtc_b200 import BBTc, BBTcError, Graph, count_batch, graphs, options
 
 pytestmark = pytest.mark.gpu
 
-KERNEL_MODES = [(k, m) for k in ("auto", "bitmap", "search", "merge") for m in ("persistent", "plain")]
+KERNEL_MODES = [(k, m) for k in ("auto", "bitmap", "search", "merge", "fused") for m in ("persistent", "plain")]
 
 
 def csr_from_edges(n, edges):
@@ -58,7 +58,7 @@ def test_buffer_and_unit_sizes(ctx, bitmap_words, unit_work):
     g = graphs.rmat(13, 24, seed=5)
     cuts = graphs.cuts(g, 6, "pal")
     want = oracle.count(g.n, g.indptr, g.indices, cuts)
-    for kernel in ("auto", "search", "merge"):
+    for kernel in ("auto", "search", "merge", "fused", "bitmap"):
         got = gpu_count(ctx, g, cuts, kernel=kernel, bitmap_words=bitmap_words, unit_work=unit_work)
         assert got == want, (kernel, bitmap_words, unit_work)
 
@@ -96,6 +96,8 @@ def test_per_task_counts(ctx):
             one = np.array([t], dtype=t.dtype)
             for kernel in ("auto", "merge"):
                 assert st.count(one, opts=options(kernel=kernel)) == want, (t, kernel)
+        with pytest.raises(BBTcError):  # fused task rows need the whole task list
+            st.count(st.task_list(), opts=options(kernel="fused"))
     finally:
         st.free()
 
@@ -261,5 +263,23 @@ def test_tile_stats_match_reference_layout(ctx):
         assert int(s["nnz"].sum()) == g.m
         info = st.info()
         assert info.n == g.n and info.m == g.m and info.P == 8
+    finally:
+        st.free()
+
+
+@pytest.mark.parametrize("bitmap_words", [16, 64, 256])
+def test_mixed_pivot_kinds_in_one_queue(ctx, bitmap_words):
+    """pal cuts give parts of very different widths, so one persistent launch
+    runs bitmap, list and global-memory pivot tasks on the same warps; the
+    shared buffer must be clean between them.  Repeated counts are identical."""
+    g = graphs.rmat(15, 16, seed=13)
+    cuts = graphs.cuts(g, 16, "pal")
+    want = oracle.count(g.n, g.indptr, g.indices, cuts)
+    st = Graph.from_csr(ctx, g, cuts)
+    try:
+        for unit_work in (64, 2048):
+            for kernel in ("auto", "bitmap"):
+                o = options(kernel=kernel, bitmap_words=bitmap_words, unit_work=unit_work, blocks_per_sm=1)
+                assert [st.count(opts=o) for _ in range(3)] == [want] * 3, (kernel, bitmap_words, unit_work)
     finally:
         st.free()
