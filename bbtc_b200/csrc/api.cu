@@ -357,6 +357,70 @@ int bbtc_last_launches(const bbtc_graph* g, uint32_t* launches) {
   return BBTC_OK;
 }
 
+int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bbtc_opts* inout, double* best_ms) {
+  if (!ctx || !g || !inout) return fail(BBTC_ERR_ARG, "NULL argument");
+  static const uint32_t kWords[] = {256, 512, 1024, 2048, 4096};
+  static const uint32_t kWarps[] = {4, 8};
+  static const uint32_t kWork[] = {2048, 8192, 32768};
+  bbtc_tune_space sp{kWords, 5, kWarps, 2, kWork, 3, 3};
+  if (space) {
+    sp = *space;
+    if (!sp.bitmap_words || !sp.n_bitmap_words) { sp.bitmap_words = kWords; sp.n_bitmap_words = 5; }
+    if (!sp.warps_per_block || !sp.n_warps_per_block) { sp.warps_per_block = kWarps; sp.n_warps_per_block = 2; }
+    if (!sp.unit_work || !sp.n_unit_work) { sp.unit_work = kWork; sp.n_unit_work = 3; }
+    if (!sp.repeats) sp.repeats = 3;
+  }
+  BBTC_CUDA(cudaSetDevice(ctx->device));
+  cudaEvent_t a, b;
+  BBTC_CUDA(cudaEventCreate(&a));
+  BBTC_CUDA(cudaEventCreate(&b));
+  struct Ev {
+    cudaEvent_t a, b;
+    ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } evs{a, b};
+  bbtc_opts best = *inout;
+  double best_t = 1e300;
+  uint64_t ref_count = 0;
+  bool have_ref = false;
+  for (uint32_t iw = 0; iw < sp.n_bitmap_words; iw++)
+    for (uint32_t ip = 0; ip < sp.n_warps_per_block; ip++)
+      for (uint32_t iu = 0; iu < sp.n_unit_work; iu++) {
+        bbtc_opts o = *inout;
+        o.bitmap_words = sp.bitmap_words[iw];
+        o.warps_per_block = sp.warps_per_block[ip];
+        o.unit_work = sp.unit_work[iu];
+        if (smem_bytes_for(o) > ctx->smem_optin) continue;  // does not fit this device
+        uint64_t c = 0;
+        BBTC_TRY(bbtc_count(ctx, g, nullptr, 0, -1, &o, &c));  // warm-up, builds the plan
+        std::vector<float> ts;
+        for (uint32_t r = 0; r < sp.repeats; r++) {
+          BBTC_CUDA(cudaEventRecord(a, ctx->stream));
+          BBTC_TRY(bbtc_count_async(ctx, g, nullptr, 0, -1, &o));
+          BBTC_CUDA(cudaEventRecord(b, ctx->stream));
+          BBTC_TRY(bbtc_count_wait(ctx, g, &c));
+          float ms = 0;
+          BBTC_CUDA(cudaEventElapsedTime(&ms, a, b));
+          ts.push_back(ms);
+          if (!have_ref) {
+            ref_count = c;
+            have_ref = true;
+          } else if (c != ref_count) {
+            return fail(BBTC_ERR_STATE, "autotune points disagree on the count");
+          }
+        }
+        std::sort(ts.begin(), ts.end());
+        const double med = ts[ts.size() / 2];
+        if (med < best_t) {
+          best_t = med;
+          best = o;
+        }
+      }
+  if (!have_ref) return fail(BBTC_ERR_ARG, "no point of the tuning space fits this device");
+  *inout = best;
+  if (best_ms) *best_ms = best_t;
+  return BBTC_OK;
+}
+
 int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, const bbtc_opts* opts, uint64_t* outs) {
   if (!ctx || (ng && (!graphs || !outs))) return fail(BBTC_ERR_ARG, "NULL argument");
   if (ng == 0) return BBTC_OK;

@@ -32,8 +32,8 @@
 // In the persistent form every warp of a grid sized to the SM count claims
 // units from one atomic head over all tasks (cost-sorted, heaviest first); in
 // the plain form each task is one launch whose warps stride over its units.
-// Inside a unit the rows met by 32 entries are concatenated and split into 32
-// equal contiguous slices (merge-path split), one per lane.
+// Inside a unit the rows met by 32 entries are concatenated and walked 32
+// consecutive ids at a time (see probe_entries).
 #include <algorithm>
 #include <cstring>
 #include <sstream>
@@ -65,15 +65,17 @@ struct PivotView {
   const uint32_t* row;  // global pivot row
   uint32_t len;
   uint32_t base;  // bitmap bit 0 <-> id `base`
-  uint32_t span;  // ids in [base, base + span) may be set
+  uint32_t cap;   // a bit of the warp's last buffer word, which stays zero
   uint32_t first, last;
 };
 
 template <uint32_t KIND>
 __device__ __forceinline__ uint32_t member(const uint32_t* bm, const PivotView& pv, uint32_t x) {
   if constexpr (KIND == kPivotBitmap) {
-    const uint32_t y = x - pv.base;
-    return y < pv.span ? (bm[y >> 5] >> (y & 31)) & 1u : 0u;
+    // ids outside the pivot's span (below base they wrap high) land on the
+    // always-zero last word: no branch
+    const uint32_t y = min(x - pv.base, pv.cap);
+    return (bm[y >> 5] >> (y & 31)) & 1u;
   } else if constexpr (KIND == kPivotList) {
     if (x < pv.first || x > pv.last) return 0;
     const uint32_t p = lower_bound_u32(bm, pv.len, x);
@@ -106,6 +108,14 @@ struct RecSegs {  // fused: the stored (start, end) of N+(u) after v
 
 // Probe the rows met by entries [e, ee) against the pivot structure; returns
 // this lane's hit count.
+//
+// The rows met by a batch of 32 entries are concatenated and walked 32 ids at
+// a time, lane l taking ids l, l + 32, l + 64, ..., so each warp load reads
+// consecutive ids.  Every lane keeps a pointer to the row that owns its
+// current id (found once per batch by bisection of the 33 row starts in
+// shared memory) and moves it forward when its id passes the row's end --
+// less than once per window on average -- so the owner costs one compare per
+// id.  Four windows are loaded before any is tested.
 template <uint32_t KIND, class Segs>
 __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, uint32_t ee,
                                                   const uint32_t* __restrict__ prb_col, const uint32_t* bm,
@@ -126,43 +136,35 @@ __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, 
     if (total == 0) continue;
     const uint32_t excl = incl - len;
     sstart[lane] = excl;
-    sbase[lane] = start - excl;  // modular: sbase + p is the id's position for p in the segment
+    sbase[lane] = start - excl;  // modular: sbase + id is the id's position for ids of this row
     if (lane == 31) sstart[32] = total;
     __syncwarp();
-    const uint32_t per = (total + 31) >> 5;
-    const uint32_t pbeg = lane * per;
-    const uint32_t pend = min(pbeg + per, total);
-    if (pbeg < pend) {
-      uint32_t owner = 0;
+    // owner of id = lane: the last row whose start is <= lane (empty rows share starts)
+    uint32_t owner = 0;
 #pragma unroll
-      for (uint32_t step = 16; step > 0; step >>= 1)
-        if (sstart[owner + step] <= pbeg) owner += step;
-      uint32_t nb = sstart[owner + 1];
-      uint32_t bs = sbase[owner];
-      uint32_t p = pbeg;
-      // four independent loads in flight per lane
-      for (; p + 4 <= pend; p += 4) {
-        uint32_t x[4];
+    for (uint32_t step = 16; step > 0; step >>= 1)
+      if (sstart[owner + step] <= lane) owner += step;
+    uint32_t nb = sstart[owner + 1];
+    uint32_t bs = sbase[owner];
+    for (uint32_t c = 0; c < total; c += 128) {
+      uint32_t x[4];
+      bool ok[4];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          while (p + k >= nb) {
+      for (int k = 0; k < 4; k++) {
+        const uint32_t id = c + 32u * k + lane;
+        ok[k] = id < total;
+        x[k] = 0;
+        if (ok[k]) {
+          while (id >= nb) {
             owner++;
             nb = sstart[owner + 1];
             bs = sbase[owner];
           }
-          x[k] = __ldg(prb_col + bs + p + k);
+          x[k] = __ldg(prb_col + bs + id);
         }
+      }
 #pragma unroll
-        for (int k = 0; k < 4; k++) hits += member<KIND>(bm, pv, x[k]);
-      }
-      for (; p < pend; p++) {
-        while (p >= nb) {
-          owner++;
-          nb = sstart[owner + 1];
-          bs = sbase[owner];
-        }
-        hits += member<KIND>(bm, pv, __ldg(prb_col + bs + p));
-      }
+      for (int k = 0; k < 4; k++) hits += ok[k] ? member<KIND>(bm, pv, x[k]) : 0u;
     }
     __syncwarp();
   }
@@ -188,7 +190,7 @@ __device__ __forceinline__ uint32_t pivot_pass(const uint32_t* __restrict__ prow
   pv.row = prow;
   pv.len = pd;
   pv.base = base;
-  pv.span = words * 32;
+  pv.cap = words * 32;  // callers keep words < the buffer size, so word `words` is never set
   pv.first = prow[0];
   pv.last = prow[pd - 1];
   const uint32_t hits = probe_entries<KIND>(segs, e, ee, prb_col, bm, sstart, sbase, pv, lane);
@@ -292,7 +294,7 @@ __device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_
       const uint32_t* prow = gi + ps;
       const uint32_t first = prow[0];
       const uint32_t span_words = ((prow[pd - 1] - first) >> 5) + 1;
-      if (span_words <= bm_words)
+      if (span_words < bm_words)
         acc += pivot_pass<kPivotBitmap>(prow, pd, first, span_words, segs, e, ee, gi, bm, sstart, sbase, lane);
       else if (pd <= bm_words)
         acc += pivot_pass<kPivotList>(prow, pd, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
@@ -379,6 +381,10 @@ uint32_t norm_warps(uint32_t w) { return w == 0 ? 8 : std::min<uint32_t>(std::ma
 
 }  // namespace
 
+size_t smem_bytes_for(const bbtc_opts& o) {
+  return smem_bytes(norm_bm_words(o.bitmap_words), norm_warps(o.warps_per_block));
+}
+
 int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o) {
   const size_t sm = smem_bytes(norm_bm_words(o.bitmap_words), norm_warps(o.warps_per_block));
   if (sm > ctx->smem_optin)
@@ -454,7 +460,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
         d.probe = dev_tile(g->fwd, g->cuts, i, k);
       }
       d.words = (d.pivot.W + 31) / 32;
-      const bool fits_bitmap = d.words <= bmw;
+      const bool fits_bitmap = d.words < bmw;  // the word after the part stays zero
       const bool fits_list = d.pivot.maxdeg <= bmw;
       if (!u_centric && o.kernel != BBTC_KERNEL_SEARCH && fits_bitmap)
         d.kind = kPivotBitmap;

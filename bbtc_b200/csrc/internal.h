@@ -133,5 +133,6 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
                   const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o, bool fused,
                   uint64_t* d_outs, Plan* plan, bool reuse);
 int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o);
+size_t smem_bytes_for(const bbtc_opts& o);
 
 }  // namespace bbtc

@@ -162,6 +162,26 @@ int bbtc_count_wait(bbtc_ctx* ctx, bbtc_graph* g, uint64_t* out);
 /* Launches of this library's kernels issued by the last count on g. */
 int bbtc_last_launches(const bbtc_graph* g, uint32_t* launches);
 
+/* ---- autotuner ------------------------------------------------------------
+ * Times the count of g under every combination of the listed shared-buffer
+ * sizes (the bitmap-vs-search threshold: a pivot row becomes a bitmap when its
+ * id span fits, else a sorted list), warps per block and work-unit sizes, and
+ * writes the fastest into *inout (mode and kernel are kept).  Every point must
+ * give the same count, else BBTC_ERR_STATE.  NULL space = the default sweep.
+ * No reference counterpart: the reference fixes its kernel choice by a width
+ * test (bb_tc.cpp:98). */
+typedef struct bbtc_tune_space {
+  const uint32_t* bitmap_words;
+  uint32_t n_bitmap_words;
+  const uint32_t* warps_per_block;
+  uint32_t n_warps_per_block;
+  const uint32_t* unit_work;
+  uint32_t n_unit_work;
+  uint32_t repeats; /* timed counts per point, the median is kept (0 = 3) */
+} bbtc_tune_space;
+int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bbtc_opts* inout,
+                  double* best_ms);
+
 /* Count many graphs in one persistent launch: every graph's TaskList(P)
  * goes into one cost-sorted device queue, each graph gets its own u64.  outs[ng]. */
 int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, const bbtc_opts* opts,
