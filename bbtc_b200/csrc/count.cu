@@ -46,6 +46,7 @@ namespace {
 
 constexpr uint32_t FULL = 0xffffffffu;
 constexpr uint32_t kSegWords = 72;  // per-warp: 33 segment starts + 32 bases (+ pad)
+constexpr uint32_t kSplitList = 128; // split pivots: room for the ids below the bitmap window
 
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t x) {
   uint32_t lo = 0;
@@ -67,6 +68,8 @@ struct PivotView {
   uint32_t base;  // bitmap bit 0 <-> id `base`
   uint32_t cap;   // a bit of the warp's last buffer word, which stays zero
   uint32_t first, last;
+  const uint32_t* res;  // split kind: the pivot ids below `base`, sorted
+  uint32_t rlen;
 };
 
 template <uint32_t KIND>
@@ -76,6 +79,14 @@ __device__ __forceinline__ uint32_t member(const uint32_t* bm, const PivotView& 
     // always-zero last word: no branch
     const uint32_t y = min(x - pv.base, pv.cap);
     return (bm[y >> 5] >> (y & 31)) & 1u;
+  } else if constexpr (KIND == kPivotSplit) {
+    if (x >= pv.base) {
+      const uint32_t y = min(x - pv.base, pv.cap);
+      return (bm[y >> 5] >> (y & 31)) & 1u;
+    }
+    if (x < pv.first) return 0;
+    const uint32_t p = lower_bound_u32(pv.res, pv.rlen, x);
+    return (p < pv.rlen && pv.res[p] == x) ? 1u : 0u;
   } else if constexpr (KIND == kPivotList) {
     if (x < pv.first || x > pv.last) return 0;
     const uint32_t p = lower_bound_u32(bm, pv.len, x);
@@ -172,15 +183,28 @@ __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, 
 }
 
 // Build the pivot structure, probe entries [e, ee), restore the buffer to zero.
+// Split kind: ids >= base go to a bitmap of `words` words, the first `rlen`
+// ids of the row (those below base) to a sorted list after the zero word.
 template <uint32_t KIND, class Segs>
 __device__ __forceinline__ uint32_t pivot_pass(const uint32_t* __restrict__ prow, uint32_t pd, uint32_t base,
-                                               uint32_t words, const Segs& segs, uint32_t e, uint32_t ee,
-                                               const uint32_t* __restrict__ prb_col, uint32_t* bm, uint32_t* sstart,
-                                               uint32_t* sbase, uint32_t lane) {
+                                               uint32_t words, uint32_t rlen, const Segs& segs, uint32_t e,
+                                               uint32_t ee, const uint32_t* __restrict__ prb_col, uint32_t* bm,
+                                               uint32_t* sstart, uint32_t* sbase, uint32_t lane) {
+  uint32_t* res = bm + words + 1;
   if constexpr (KIND == kPivotBitmap) {
     for (uint32_t i = lane; i < pd; i += 32) {
       const uint32_t y = prow[i] - base;
       atomicOr(&bm[y >> 5], 1u << (y & 31));
+    }
+  } else if constexpr (KIND == kPivotSplit) {
+    for (uint32_t i = lane; i < pd; i += 32) {
+      const uint32_t x = prow[i];
+      if (i < rlen) {
+        res[i] = x;
+      } else {
+        const uint32_t y = x - base;
+        atomicOr(&bm[y >> 5], 1u << (y & 31));
+      }
     }
   } else if constexpr (KIND == kPivotList) {
     for (uint32_t i = lane; i < pd; i += 32) bm[i] = prow[i];
@@ -193,6 +217,8 @@ __device__ __forceinline__ uint32_t pivot_pass(const uint32_t* __restrict__ prow
   pv.cap = words * 32;  // callers keep words < the buffer size, so word `words` is never set
   pv.first = prow[0];
   pv.last = prow[pd - 1];
+  pv.res = res;
+  pv.rlen = rlen;
   const uint32_t hits = probe_entries<KIND>(segs, e, ee, prb_col, bm, sstart, sbase, pv, lane);
   // the buffer is all-zero between pivots whatever kind used it last: the
   // persistent queue hands one warp bitmap and list work in any order
@@ -203,6 +229,13 @@ __device__ __forceinline__ uint32_t pivot_pass(const uint32_t* __restrict__ prow
     } else {
       for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
     }
+  } else if constexpr (KIND == kPivotSplit) {
+    if (pd - rlen < words) {
+      for (uint32_t i = lane + rlen; i < pd; i += 32) bm[(prow[i] - base) >> 5] = 0;
+    } else {
+      for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
+    }
+    for (uint32_t i = lane; i < rlen; i += 32) res[i] = 0;
   } else if constexpr (KIND == kPivotList) {
     for (uint32_t i = lane; i < pd; i += 32) bm[i] = 0;
   }
@@ -255,13 +288,14 @@ __device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t
       const uint32_t* prow = p_col + ps;
       switch (tk.kind) {
         case kPivotBitmap:
-          acc += pivot_pass<kPivotBitmap>(prow, pd, 0, tk.words, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotBitmap>(prow, pd, 0, tk.words, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase,
+                                          lane);
           break;
         case kPivotList:
-          acc += pivot_pass<kPivotList>(prow, pd, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotList>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
           break;
         default:
-          acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
       }
     }
     e = ee;
@@ -293,13 +327,22 @@ __device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_
     if (pd > 0) {
       const uint32_t* prow = gi + ps;
       const uint32_t first = prow[0];
-      const uint32_t span_words = ((prow[pd - 1] - first) >> 5) + 1;
-      if (span_words < bm_words)
-        acc += pivot_pass<kPivotBitmap>(prow, pd, first, span_words, segs, e, ee, gi, bm, sstart, sbase, lane);
-      else if (pd <= bm_words)
-        acc += pivot_pass<kPivotList>(prow, pd, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
-      else
-        acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+      const uint32_t last = prow[pd - 1];
+      const uint32_t span_words = ((last - first) >> 5) + 1;
+      if (span_words < bm_words) {
+        acc += pivot_pass<kPivotBitmap>(prow, pd, first, span_words, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+      } else {
+        // bitmap over the top window of the row, the few ids below it in a short list
+        const uint32_t wwords = bm_words - 1 - kSplitList;
+        const uint32_t wbase = last - (wwords * 32 - 1);
+        const uint32_t rlen = lower_bound_u32(prow, pd, wbase);
+        if (rlen <= kSplitList)
+          acc += pivot_pass<kPivotSplit>(prow, pd, wbase, wwords, rlen, segs, e, ee, gi, bm, sstart, sbase, lane);
+        else if (pd <= bm_words)
+          acc += pivot_pass<kPivotList>(prow, pd, 0, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+        else
+          acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+      }
     }
     e = ee;
     if (e < e1) b = next_row(r_rp, H, b, e, lane);
@@ -374,7 +417,7 @@ size_t smem_bytes(uint32_t bm_words, uint32_t warps) {
 uint32_t norm_bm_words(uint32_t w) {
   if (w == 0) w = 1024;
   w = (w + 3) & ~3u;
-  return std::max<uint32_t>(w, 32);
+  return std::max<uint32_t>(w, 2 * kSplitList);
 }
 
 uint32_t norm_warps(uint32_t w) { return w == 0 ? 8 : std::min<uint32_t>(std::max<uint32_t>(w, 1), 8); }

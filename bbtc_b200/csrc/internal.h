@@ -49,6 +49,7 @@ enum TaskKind : uint32_t {
   kPivotList = 1,    // pivot row -> sorted shared list, probes binary-search it
   kPivotGlobal = 2,  // pivot row too long for shared memory: binary search in global memory
   kFusedRow = 3,     // task row (i, j): all tasks (i, j, k >= j) in one pass, structure chosen per pivot
+  kPivotSplit = 4,   // pivot row -> bitmap of its top id window + short sorted list of the ids below it
 };
 
 // One queued task: `rows` is the tile whose rows are the pivot vertices and
