@@ -35,7 +35,9 @@
 // Inside a unit the rows met by 32 entries are concatenated and walked 32
 // consecutive ids at a time (see probe_entries).
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
+#include <mutex>
 #include <sstream>
 
 #include "internal.h"
@@ -618,4 +620,199 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
   return BBTC_OK;
 }
 
+// ---- counting without allocation --------------------------------------------
+//
+// bbtc_count_csr_noalloc counts the triangles of an oriented CSR that the
+// caller already holds in device memory, for callers that cannot allocate
+// device memory themselves or through this library: code that runs inside
+// another framework's device-memory manager (which owns the device's memory
+// and hands out only slices of its own pool), processes held to a fixed
+// device-memory quota, and paths that must not pay cudaMalloc / cudaFree's
+// implicit device synchronisation.  It is the persistent queue kernel's
+// scheme run over the CSR as one task (P = 1, the reference's row order: the
+// pivot is N+(u), the rows streamed are N+(v) for v in N+(u)); every word of
+// scratch -- the queue head, an error word, the total and one partial count
+// per work unit -- lives in the static array below, so the call allocates
+// nothing.  Limit: at most kNoAllocMaxEdges oriented edges.
+constexpr uint32_t kNoAllocUnitEdges = 256;
+constexpr uint64_t kNoAllocMaxEdges = 1ull << 24;  // 16,777,216 oriented edges
+constexpr uint32_t kNoAllocMaxUnits = (uint32_t)(kNoAllocMaxEdges / kNoAllocUnitEdges);
+
+struct NoAllocScratch {
+  uint32_t head;   // next work unit
+  uint32_t error;  // bit 0: a row pointer or id outside the CSR was met
+  unsigned long long total;
+  uint32_t pad[60];
+  unsigned long long partial[kNoAllocMaxUnits];
+};
+
+// One copy per device that loads the library, kept until the process exits
+// (about 512 KiB).  Host code must not take its address directly: the
+// device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+namespace {
+
+// Row ranges of a caller CSR, checked against [0, m] and ids against n.
+struct CheckedCsrSegs {
+  const uint32_t* __restrict__ col;
+  const uint32_t* __restrict__ rp;
+  uint32_t n;
+  uint64_t m;
+  uint32_t* err;
+  __device__ __forceinline__ void get(uint32_t q, uint32_t& start, uint32_t& len) const {
+    const uint32_t v = col[q];
+    start = 0;
+    len = 0;
+    if (v >= n) {
+      atomicOr(err, 1u);
+      return;
+    }
+    const uint32_t a = rp[v], b = rp[v + 1];
+    if (b < a || (uint64_t)b > m) {
+      atomicOr(err, 1u);
+      return;
+    }
+    start = a;
+    len = b - a;
+  }
+};
+
+__global__ void __launch_bounds__(256, 4) k_count_csr_static(const uint32_t* __restrict__ indptr,
+                                                             const uint32_t* __restrict__ indices, uint32_t n,
+                                                             uint64_t m, uint32_t units, NoAllocScratch* scr,
+                                                             uint32_t bm_words) {
+  extern __shared__ __align__(16) uint32_t sh[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* bm = sh + warp * (bm_words + kSegWords);
+  uint32_t* sstart = bm + bm_words;
+  uint32_t* sbase = sstart + 33;
+  for (uint32_t i = lane; i < bm_words; i += 32) bm[i] = 0;
+  __syncwarp();
+  const CheckedCsrSegs segs{indices, indptr, n, m, &scr->error};
+  while (true) {
+    uint32_t g = 0;
+    if (lane == 0) g = atomicAdd(&scr->head, 1u);
+    g = __shfl_sync(FULL, g, 0);
+    if (g >= units) break;
+    const uint32_t e0 = g * kNoAllocUnitEdges;
+    const uint64_t e1w = (uint64_t)e0 + kNoAllocUnitEdges;
+    const uint32_t e1 = (uint32_t)(e1w < m ? e1w : m);
+    uint32_t e = e0;
+    uint32_t u = row_of(indptr, n, e);
+    unsigned long long acc = 0;
+    while (e < e1) {
+      const uint32_t a = indptr[u], b = indptr[u + 1];
+      if (b < a || (uint64_t)b > m || b <= e) {  // malformed row pointers: stop this unit
+        if (lane == 0) atomicOr(&scr->error, 1u);
+        break;
+      }
+      const uint32_t ee = min(b, e1);
+      const uint32_t pd = b - a;
+      const uint32_t* prow = indices + a;
+      // the caller's row must be strictly increasing: the bitmap is indexed by id
+      bool sorted = true;
+      for (uint32_t i = lane; i + 1 < pd; i += 32) sorted &= prow[i] < prow[i + 1];
+      if (!__all_sync(FULL, sorted)) {
+        if (lane == 0) atomicOr(&scr->error, 1u);
+        e = ee;
+        if (e < e1) u = next_row(indptr, n, u, e, lane);
+        continue;
+      }
+      const uint32_t first = prow[0], last = prow[pd - 1];
+      const uint32_t span_words = last >= first ? ((last - first) >> 5) + 1 : 0xffffffffu;
+      if (span_words < bm_words)
+        acc += pivot_pass<kPivotBitmap>(prow, pd, first, span_words, 0, segs, e, ee, indices, bm, sstart, sbase,
+                                        lane);
+      else if (pd <= bm_words)
+        acc += pivot_pass<kPivotList>(prow, pd, 0, 0, 0, segs, e, ee, indices, bm, sstart, sbase, lane);
+      else
+        acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, 0, segs, e, ee, indices, bm, sstart, sbase, lane);
+      e = ee;
+      if (e < e1) u = next_row(indptr, n, u, e, lane);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) scr->partial[g] = acc;
+  }
+}
+
+// total = sum of the unit partials, in a fixed order (one block).
+__global__ void k_noalloc_total(NoAllocScratch* scr, uint32_t units) {
+  __shared__ unsigned long long part[1024];
+  unsigned long long s = 0;
+  for (uint32_t i = threadIdx.x; i < units; i += blockDim.x) s += scr->partial[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (uint32_t w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) scr->total = part[0];
+}
+
+}  // namespace
+
+namespace {
+
+// Device address of g_noalloc_scratch, looked up once per device.
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+}  // namespace
+
 }  // namespace bbtc
+
+extern "C" int bbtc_count_csr_noalloc(const uint32_t* d_indptr, const uint32_t* d_indices, uint32_t n, uint64_t m,
+                                      uint64_t* out, void* stream) {
+  using namespace bbtc;
+  if (!d_indptr || (m && !d_indices) || !out) return fail(BBTC_ERR_ARG, "NULL argument");
+  if (n == 0xffffffffu) return fail(BBTC_ERR_ARG, "n must be below 2^32 - 1");
+  if (m > kNoAllocMaxEdges)
+    return fail(BBTC_ERR_CAPACITY, "bbtc_count_csr_noalloc takes at most " + std::to_string(kNoAllocMaxEdges) +
+                                       " oriented edges (its static scratch has one slot per 256 edges); got " +
+                                       std::to_string(m));
+  int dev = 0;
+  BBTC_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= (int)kMaxDevices) return fail(BBTC_ERR_NODEV, "device index beyond the supported range");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  void* ptr = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      // first call on this device (which is current): resolve the array's device address
+      const cudaError_t e = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
+      if (e != cudaSuccess) {
+        g_noalloc_ptr[dev] = nullptr;
+        return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+      }
+    }
+    ptr = g_noalloc_ptr[dev];
+  }
+  NoAllocScratch* scr = static_cast<NoAllocScratch*>(ptr);
+  // head, error and total start at zero; the partials of this call's units are all rewritten
+  BBTC_CUDA(cudaMemsetAsync(scr, 0, offsetof(NoAllocScratch, pad), s));
+  const uint32_t units = (uint32_t)((m + kNoAllocUnitEdges - 1) / kNoAllocUnitEdges);
+  if (units > 0) {
+    const uint32_t bmw = 1024, wpb = 8;
+    const size_t sm = smem_bytes(bmw, wpb);
+    BBTC_CUDA(cudaFuncSetAttribute(k_count_csr_static, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int sms = 0, per_sm = 0;
+    BBTC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count_csr_static, wpb * 32, sm));
+    const uint32_t grid = (uint32_t)std::max(1, sms * std::max(1, per_sm));
+    k_count_csr_static<<<grid, wpb * 32, sm, s>>>(d_indptr, d_indices, n, m, units, scr, bmw);
+    BBTC_CUDA(cudaGetLastError());
+    k_noalloc_total<<<1, 1024, 0, s>>>(scr, units);
+    BBTC_CUDA(cudaGetLastError());
+  }
+  struct {
+    uint32_t head, error;
+    unsigned long long total;
+  } hdr{0, 0, 0};
+  BBTC_CUDA(cudaMemcpyAsync(&hdr, scr, sizeof(hdr), cudaMemcpyDeviceToHost, s));
+  BBTC_CUDA(cudaStreamSynchronize(s));
+  if (hdr.error) return fail(BBTC_ERR_INPUT, "the CSR has a row pointer or column id outside its bounds, or an "
+                                            "unsorted row");
+  *out = hdr.total;
+  return BBTC_OK;
+}

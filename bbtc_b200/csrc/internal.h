@@ -31,6 +31,7 @@ int cuda_fail(cudaError_t e, const char* what);
   } while (0)
 
 constexpr uint32_t kMaxParts = 64;
+constexpr uint32_t kMaxDevices = 64;
 constexpr uint64_t kNoSegment = ~0ull;
 
 // One tile as the kernels see it: tile-local row pointers (H+1 entries, the

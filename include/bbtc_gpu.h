@@ -187,6 +187,29 @@ int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bb
 int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, const bbtc_opts* opts,
                      uint64_t* outs);
 
+/* ---- counting without allocation -------------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory -- code running inside another framework's
+ * device-memory manager that owns the device's memory and hands out only
+ * slices of its own pool, processes held to a fixed device-memory quota, and
+ * paths that must not pay the implicit device synchronisation of cudaMalloc /
+ * cudaFree.  The caller passes a degree-ordered, oriented CSR that is already
+ * in device memory of the current device (d_indptr[n+1], d_indices[m], rows
+ * strictly increasing) and a host pointer for the count; the call allocates
+ * nothing.  Its scratch (queue head, error word, total, one partial count per
+ * 256 edges) is a file-scope device array of about 512 KiB that every GPU
+ * loading the library holds until the process exits, so m is limited to
+ * 16,777,216 oriented edges (larger m: BBTC_ERR_CAPACITY, nothing launched).
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array and it
+ * keeps the last call's contents: each call clears what must start at zero,
+ * and calls that overlap on the GPU (on different streams or threads) race --
+ * serialise them.  Work is enqueued on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream) and the call waits for it.  A row pointer or id out
+ * of bounds, or an unsorted row, is reported as BBTC_ERR_INPUT. */
+int bbtc_count_csr_noalloc(const uint32_t* d_indptr, const uint32_t* d_indices, uint32_t n, uint64_t m,
+                           uint64_t* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
