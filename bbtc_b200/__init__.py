@@ -5,8 +5,8 @@ include/bbtc_gpu.h; this package binds it (``core``), generates seeded input
 graphs and cut vectors (``graphs``, host library libbbtc_host.so) and builds
 everything in-tree (``build``).
 """
-from .core import (BBTc, BBTcError, Context, Graph, KERNELS, MODES, Opts, count_batch, options,  # noqa: F401
+from .core import (BBTc, BBTcError, Context, Graph, KERNELS, MODES, Opts, Server, count_batch, options,  # noqa: F401
                    task_list)
 
-__all__ = ["BBTc", "BBTcError", "Context", "Graph", "KERNELS", "MODES", "Opts", "count_batch", "options",
+__all__ = ["BBTc", "BBTcError", "Context", "Graph", "KERNELS", "MODES", "Opts", "Server", "count_batch", "options",
            "task_list"]

@@ -343,3 +343,179 @@ class BBTc:
 
     def CleanUp(self) -> None:
         self.st.free()
+
+
+# ---- request server (continuous batching) ----------------------------------
+class ServerOpts(c.Structure):
+    _fields_ = [("hbm_budget", c.c_uint64), ("max_batch", c.c_uint32), ("max_requests", c.c_uint32),
+                ("loaders", c.c_uint32), ("reserved", c.c_uint32), ("count", Opts)]
+
+
+class RequestInfo(c.Structure):
+    _fields_ = [("count", c.c_uint64), ("status", c.c_int32), ("batch", c.c_uint32), ("submit_ns", c.c_uint64),
+                ("done_ns", c.c_uint64)]
+
+
+class ServerStats(c.Structure):
+    _fields_ = [("launches", c.c_uint64), ("counted", c.c_uint64), ("max_batch", c.c_uint64),
+                ("pending", c.c_uint64), ("ready", c.c_uint64), ("device_bytes_in_use", c.c_uint64)]
+
+
+def _server_lib():
+    L = lib()
+    if getattr(L, "_server_typed", False):
+        return L
+    vp = c.c_void_p
+    L.bbtc_server_opts_default.argtypes = [c.POINTER(ServerOpts)]
+    L.bbtc_server_opts_default.restype = None
+    for name, args in {
+        "bbtc_server_create": [c.c_int, c.POINTER(ServerOpts), c.POINTER(vp)],
+        "bbtc_server_destroy": [vp],
+        "bbtc_submit": [vp, c.c_uint32, vp, vp, c.c_uint64, vp, c.c_uint32, c.POINTER(c.c_uint64)],
+        "bbtc_poll": [vp, c.c_uint64, c.POINTER(RequestInfo)],
+        "bbtc_wait": [vp, c.c_uint64, c.c_int64, c.POINTER(RequestInfo)],
+        "bbtc_release": [vp, c.c_uint64],
+        "bbtc_server_stats_get": [vp, c.POINTER(ServerStats)],
+    }.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = c.c_int
+    L._server_typed = True
+    return L
+
+
+class Server:
+    """Continuous-batching count server (bbtc_server_*).  The host CSR arrays
+    of a request are kept referenced here until the request is released."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch: int = 0, loaders: int = 0,
+                 opts: Opts | None = None):
+        L = _server_lib()
+        so = ServerOpts()
+        L.bbtc_server_opts_default(c.byref(so))
+        if hbm_budget:
+            so.hbm_budget = hbm_budget
+        if max_batch:
+            so.max_batch = max_batch
+        if loaders:
+            so.loaders = loaders
+        if opts is not None:
+            so.count = opts
+        self._h = c.c_void_p()
+        check(L.bbtc_server_create(device, c.byref(so), c.byref(self._h)))
+        self._keep: dict[int, tuple] = {}
+
+    def submit(self, n: int, indptr, indices, cuts) -> int:
+        indptr, indices, cuts = _u32(indptr), _u32(indices), _u32(cuts)
+        rid = c.c_uint64()
+        check(_server_lib().bbtc_submit(self._h, n, indptr.ctypes.data,
+                                        indices.ctypes.data if indices.size else None, indices.size,
+                                        cuts.ctypes.data, len(cuts) - 1, c.byref(rid)))
+        self._keep[rid.value] = (indptr, indices)
+        return rid.value
+
+    def submit_csr(self, csr, cuts) -> int:
+        return self.submit(csr.n, csr.indptr, csr.indices, cuts)
+
+    def poll(self, rid: int) -> RequestInfo:
+        info = RequestInfo()
+        check(_server_lib().bbtc_poll(self._h, rid, c.byref(info)))
+        return info
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> RequestInfo:
+        info = RequestInfo()
+        check(_server_lib().bbtc_wait(self._h, rid, timeout_ms, c.byref(info)))
+        return info
+
+    def release(self, rid: int) -> None:
+        check(_server_lib().bbtc_release(self._h, rid))
+        self._keep.pop(rid, None)
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(_server_lib().bbtc_server_stats_get(self._h, c.byref(st)))
+        return st
+
+    def close(self) -> None:
+        if self._h:
+            _server_lib().bbtc_server_destroy(self._h)
+            self._h = c.c_void_p()
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- device-side input preparation -------------------------------------------
+class CsrDev(c.Structure):
+    _fields_ = [("indptr", c.c_void_p), ("indices", c.c_void_p), ("n", c.c_uint32), ("m", c.c_uint64)]
+
+
+def _prep_lib():
+    L = lib()
+    if getattr(L, "_prep_typed", False):
+        return L
+    vp = c.c_void_p
+    for name, args in {
+        "bbtc_rmat_device": [vp, c.c_int, c.c_int, c.c_double, c.c_double, c.c_double, c.c_uint64, vp, vp],
+        "bbtc_orient_device": [vp, c.c_uint32, vp, vp, c.c_uint64, c.POINTER(CsrDev)],
+        "bbtc_csr_dev_free": [vp, c.POINTER(CsrDev)],
+    }.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = c.c_int
+    L._prep_typed = True
+    return L
+
+
+def rmat_device(ctx: Context, scale: int, edge_factor: int, d_src: int, d_dst: int, seed: int,
+                a: float = 0.57, b: float = 0.19, cc: float = 0.19) -> None:
+    """Fill device buffers (edge_factor << scale entries each) with R-MAT pairs."""
+    check(_prep_lib().bbtc_rmat_device(ctx.handle, scale, edge_factor, a, b, cc, seed, d_src, d_dst))
+
+
+class DeviceCSR:
+    """An oriented CSR built on the device by bbtc_orient_device."""
+
+    def __init__(self, ctx: Context, n: int, d_src: int, d_dst: int, m_raw: int):
+        self.ctx = ctx
+        self._c = CsrDev()
+        check(_prep_lib().bbtc_orient_device(ctx.handle, n, d_src, d_dst, m_raw, c.byref(self._c)))
+
+    @property
+    def n(self) -> int:
+        return self._c.n
+
+    @property
+    def m(self) -> int:
+        return self._c.m
+
+    @property
+    def indptr_ptr(self) -> int:
+        return self._c.indptr
+
+    @property
+    def indices_ptr(self) -> int:
+        return self._c.indices
+
+    def graph(self, cuts) -> Graph:
+        return Graph.upload_device(self.ctx, self.n, self.indptr_ptr, self.indices_ptr, self.m, cuts)
+
+    def free(self) -> None:
+        if self._c.indptr:
+            _prep_lib().bbtc_csr_dev_free(self.ctx.handle, c.byref(self._c))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

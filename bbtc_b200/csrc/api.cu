@@ -79,7 +79,7 @@ int finish_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* indptr, const uint3
   g->m = m;
   g->P = P;
   g->cuts.assign(cuts, cuts + P + 1);
-  if (cudaMalloc(&g->d_count, 64 * sizeof(uint64_t)) != cudaSuccess) {
+  if (cudaMallocAsync(&g->d_count, 64 * sizeof(uint64_t), ctx->stream) != cudaSuccess) {
     cudaGetLastError();
     delete g;
     return fail(BBTC_ERR_NOMEM, "device allocation of the result slot failed");
@@ -94,6 +94,20 @@ int finish_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* indptr, const uint3
 }
 
 }  // namespace
+
+// Free a graph's device memory on stream s (the caller has made sure nothing
+// on the device still reads it) without waiting for the graph's own stream.
+void graph_release_on(bbtc_graph* g, cudaStream_t s) {
+  if (!g) return;
+  for (auto& kv : g->plans) kv.second->release();
+  g->fwd.release(s);
+  g->rev.release(s);
+  if (g->d_indptr) cudaFreeAsync(g->d_indptr, s);
+  if (g->d_indices) cudaFreeAsync(g->d_indices, s);
+  if (g->d_count) cudaFreeAsync(g->d_count, s);
+  delete g;
+}
+
 }  // namespace bbtc
 
 using namespace bbtc;
@@ -207,8 +221,8 @@ int bbtc_graph_free(bbtc_graph* g) {
   g->rev.release(s);
   if (g->d_indptr) cudaFreeAsync(g->d_indptr, s);
   if (g->d_indices) cudaFreeAsync(g->d_indices, s);
+  if (g->d_count) cudaFreeAsync(g->d_count, s);
   cudaStreamSynchronize(s);
-  if (g->d_count) cudaFree(g->d_count);
   delete g;
   return BBTC_OK;
 }
@@ -436,11 +450,12 @@ int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, cons
     tl[i] = default_tasks(gs[i], o.sort_tasks != 0);
   }
   uint64_t* d_outs = nullptr;
-  BBTC_CUDA(cudaMalloc(&d_outs, ng * sizeof(uint64_t)));
+  BBTC_CUDA(cudaMallocAsync(&d_outs, ng * sizeof(uint64_t), ctx->stream));
   struct F {
     uint64_t* p;
-    ~F() { cudaFree(p); }
-  } guard{d_outs};
+    cudaStream_t s;
+    ~F() { cudaFreeAsync(p, s); }
+  } guard{d_outs, ctx->stream};
   Plan plan;
   o.use_cuda_graph = 0;
   // one queue for all graphs: tasks of every graph merged by cost, heaviest first

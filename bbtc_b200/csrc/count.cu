@@ -537,11 +537,12 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
 
 void Plan::release() {
   if (exec) cudaGraphExecDestroy(exec);
-  if (d_tasks) cudaFree(d_tasks);
-  if (d_prefix) cudaFree(d_prefix);
+  if (d_tasks) cudaFreeAsync(d_tasks, stream);
+  if (d_prefix) cudaFreeAsync(d_prefix, stream);
   exec = nullptr;
   d_tasks = nullptr;
   d_prefix = nullptr;
+  cap = 0;
 }
 
 static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint64_t* d_outs, uint32_t nouts) {
@@ -583,15 +584,22 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
   cudaStream_t s = ctx->stream;
   BBTC_TRY(kernel_smem_optin(ctx, o));
   if (!reuse) {
-    plan->release();
+    if (plan->exec) cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
     BBTC_TRY(make_plan(graphs, tasks, o, fused, plan));
     const size_t nt = plan->tasks.size();
     if (nt) {
-      if (cudaMalloc(&plan->d_tasks, nt * sizeof(DevTask)) != cudaSuccess ||
-          cudaMalloc(&plan->d_prefix, (nt + 1) * sizeof(uint32_t)) != cudaSuccess) {
-        cudaGetLastError();
+      if (nt > plan->cap || plan->stream != s) {
         plan->release();
-        return fail(BBTC_ERR_NOMEM, "device allocation of the task queue failed");
+        plan->stream = s;
+        const size_t cap = std::max<size_t>(nt, 256);
+        if (cudaMallocAsync(&plan->d_tasks, cap * sizeof(DevTask), s) != cudaSuccess ||
+            cudaMallocAsync(&plan->d_prefix, (cap + 1) * sizeof(uint32_t), s) != cudaSuccess) {
+          cudaGetLastError();
+          plan->release();
+          return fail(BBTC_ERR_NOMEM, "device allocation of the task queue failed");
+        }
+        plan->cap = cap;
       }
       BBTC_CUDA(cudaMemcpyAsync(plan->d_tasks, plan->tasks.data(), nt * sizeof(DevTask), cudaMemcpyHostToDevice, s));
       BBTC_CUDA(cudaMemcpyAsync(plan->d_prefix, plan->prefix.data(), (nt + 1) * sizeof(uint32_t),

@@ -88,8 +88,10 @@ struct BlockTiles {
 struct Plan {
   std::vector<DevTask> tasks;      // host copy
   std::vector<uint32_t> prefix;    // unit prefix, ntasks + 1
-  DevTask* d_tasks = nullptr;
+  DevTask* d_tasks = nullptr;      // stream-ordered, reused while large enough
   uint32_t* d_prefix = nullptr;
+  size_t cap = 0;                  // tasks the device buffers hold
+  cudaStream_t stream = nullptr;   // stream the buffers were allocated on
   uint32_t total_units = 0;
   uint32_t launches = 0;
   cudaGraphExec_t exec = nullptr;

@@ -187,6 +187,71 @@ int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bb
 int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, const bbtc_opts* opts,
                      uint64_t* outs);
 
+/* ---- device-side input preparation ------------------------------------------
+ * The reference prepares the counting graph on the host: symmetrise, drop
+ * self-loops (include/utils/utils.hpp:172-250), relabel by ascending degree
+ * and keep the upper triangle (SARMA csr_matrix.hpp:503-584).
+ * bbtc_orient_device does it on the GPU for m_raw pairs already in device
+ * memory (ids >= n and repeated pairs are dropped; degree ties go by id), and
+ * returns a library-allocated oriented CSR that bbtc_graph_upload_device
+ * takes; free it with bbtc_csr_dev_free.  bbtc_rmat_device fills d_src /
+ * d_dst (edge_factor << scale entries each) with R-MAT pairs drawn from the
+ * same counter-based stream as the host generator, so both give the same
+ * graph for the same seed. */
+typedef struct bbtc_csr_dev {
+  uint32_t* indptr;  /* n + 1 */
+  uint32_t* indices; /* m */
+  uint32_t n;
+  uint64_t m;
+} bbtc_csr_dev;
+int bbtc_rmat_device(bbtc_ctx* ctx, int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                     uint32_t* d_src, uint32_t* d_dst);
+int bbtc_orient_device(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m_raw,
+                       bbtc_csr_dev* out);
+int bbtc_csr_dev_free(bbtc_ctx* ctx, bbtc_csr_dev* csr);
+
+/* ---- request server: continuous batching ----------------------------------
+ * No counterpart in the reference (one graph per process).  Loader threads
+ * build each submitted graph's device block CSR on their own streams,
+ * admitting requests in arrival order while their estimated device footprint
+ * fits hbm_budget; one launcher thread counts every ready graph in a single
+ * persistent launch (one u64 slot per graph), publishes the counts and frees
+ * the graphs.  Requests that arrive while a launch runs are loaded meanwhile
+ * and join the next launch.  All server calls are thread-safe.  The caller's
+ * indptr / indices must stay valid until the request finishes (pinned host
+ * memory makes the upload asynchronous); cuts are copied. */
+typedef struct bbtc_server bbtc_server;
+typedef struct bbtc_server_opts {
+  uint64_t hbm_budget;    /* device bytes admitted graphs may hold (0 = 150 GiB) */
+  uint32_t max_batch;     /* graphs per launch (0 = 4096) */
+  uint32_t max_requests;  /* requests held (queued, running or finished, not released) (0 = 2^20) */
+  uint32_t loaders;       /* loader threads, each with its own stream (0 = 2) */
+  uint32_t reserved;
+  bbtc_opts count;        /* launch options of every batch */
+} bbtc_server_opts;
+typedef struct bbtc_request_info {
+  uint64_t count;     /* exact count once status == 1 */
+  int32_t status;     /* 0 in flight, 1 done, < 0 failed with that bbtc_status */
+  uint32_t batch;     /* graphs in the launch that counted it */
+  uint64_t submit_ns; /* steady-clock time of bbtc_submit */
+  uint64_t done_ns;   /* steady-clock time the count reached host memory */
+} bbtc_request_info;
+typedef struct bbtc_server_stats {
+  uint64_t launches, counted, max_batch, pending, ready, device_bytes_in_use;
+} bbtc_server_stats;
+void bbtc_server_opts_default(bbtc_server_opts* o);
+int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** out);
+/* Finishes loads in progress and ready graphs; requests still queued fail with BBTC_ERR_STATE. */
+int bbtc_server_destroy(bbtc_server* s);
+int bbtc_submit(bbtc_server* s, uint32_t n, const uint32_t* indptr, const uint32_t* indices, uint64_t m,
+                const uint32_t* cuts, uint32_t P, uint64_t* req_id);
+int bbtc_poll(bbtc_server* s, uint64_t req_id, bbtc_request_info* info);
+/* timeout_ms < 0 waits for ever; BBTC_ERR_TIMEOUT if the request is still in flight */
+int bbtc_wait(bbtc_server* s, uint64_t req_id, int64_t timeout_ms, bbtc_request_info* info);
+/* Forget a finished request (its id becomes unknown). */
+int bbtc_release(bbtc_server* s, uint64_t req_id);
+int bbtc_server_stats_get(bbtc_server* s, bbtc_server_stats* st);
+
 /* ---- counting without allocation -------------------------------------------
  * No counterpart in the reference: an extra entry point for callers that
  * cannot allocate device memory -- code running inside another framework's
