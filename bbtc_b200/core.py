@@ -353,7 +353,8 @@ class ServerOpts(c.Structure):
 
 class RequestInfo(c.Structure):
     _fields_ = [("count", c.c_uint64), ("status", c.c_int32), ("batch", c.c_uint32), ("submit_ns", c.c_uint64),
-                ("done_ns", c.c_uint64)]
+                ("done_ns", c.c_uint64), ("load_ns", c.c_uint64), ("ready_ns", c.c_uint64),
+                ("launch_ns", c.c_uint64)]
 
 
 class ServerStats(c.Structure):

@@ -104,6 +104,8 @@ void graph_release_on(bbtc_graph* g, cudaStream_t s) {
   g->rev.release(s);
   if (g->d_indptr) cudaFreeAsync(g->d_indptr, s);
   if (g->d_indices) cudaFreeAsync(g->d_indices, s);
+  if (g->d_words) cudaFreeAsync(g->d_words, s);
+  if (g->d_wptr) cudaFreeAsync(g->d_wptr, s);
   if (g->d_count) cudaFreeAsync(g->d_count, s);
   delete g;
 }
@@ -221,6 +223,8 @@ int bbtc_graph_free(bbtc_graph* g) {
   g->rev.release(s);
   if (g->d_indptr) cudaFreeAsync(g->d_indptr, s);
   if (g->d_indices) cudaFreeAsync(g->d_indices, s);
+  if (g->d_words) cudaFreeAsync(g->d_words, s);
+  if (g->d_wptr) cudaFreeAsync(g->d_wptr, s);
   if (g->d_count) cudaFreeAsync(g->d_count, s);
   cudaStreamSynchronize(s);
   delete g;

@@ -100,6 +100,29 @@ __device__ __forceinline__ uint32_t member(const uint32_t* bm, const PivotView& 
   }
 }
 
+// Hits of one word-compressed pair (32-id word w.x, bit mask w.y).  The
+// bitmap kinds use a word-aligned base, so a pair meets one bitmap word; ids
+// below a split pivot's window, and the list kinds, test the set bits one by one.
+template <uint32_t KIND>
+__device__ __forceinline__ uint32_t member_word(const uint32_t* bm, const PivotView& pv, uint2 w) {
+  if constexpr (KIND == kPivotBitmap) {
+    const uint32_t yw = min(w.x - (pv.base >> 5), pv.cap >> 5);
+    return __popc(w.y & bm[yw]);
+  } else {
+    if constexpr (KIND == kPivotSplit) {
+      if (w.x >= (pv.base >> 5)) return __popc(w.y & bm[min(w.x - (pv.base >> 5), pv.cap >> 5)]);
+    }
+    uint32_t hits = 0;
+    uint32_t mask = w.y;
+    while (mask) {
+      const uint32_t x = (w.x << 5) | (uint32_t)(__ffs(mask) - 1);
+      mask &= mask - 1;
+      hits += member<KIND>(bm, pv, x);
+    }
+    return hits;
+  }
+}
+
 // Segment of the probe ids met by entry q of the rows tile.
 struct TileSegs {  // per task: the probe tile's row r = rows.col[q]
   const uint32_t* __restrict__ rcol;
@@ -129,7 +152,7 @@ struct RecSegs {  // fused: the stored (start, end) of N+(u) after v
 // shared memory) and moves it forward when its id passes the row's end --
 // less than once per window on average -- so the owner costs one compare per
 // id.  Four windows are loaded before any is tested.
-template <uint32_t KIND, class Segs>
+template <uint32_t KIND, bool WORDS, class Segs>
 __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, uint32_t ee,
                                                   const uint32_t* __restrict__ prb_col, const uint32_t* bm,
                                                   uint32_t* sstart, uint32_t* sbase, const PivotView& pv,
@@ -160,24 +183,46 @@ __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, 
     uint32_t nb = sstart[owner + 1];
     uint32_t bs = sbase[owner];
     for (uint32_t c = 0; c < total; c += 128) {
-      uint32_t x[4];
-      bool ok[4];
+      if constexpr (WORDS) {
+        const uint2* __restrict__ words = reinterpret_cast<const uint2*>(prb_col);
+        uint2 x[4];
+        bool ok[4];
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const uint32_t id = c + 32u * k + lane;
-        ok[k] = id < total;
-        x[k] = 0;
-        if (ok[k]) {
-          while (id >= nb) {
-            owner++;
-            nb = sstart[owner + 1];
-            bs = sbase[owner];
+        for (int k = 0; k < 4; k++) {
+          const uint32_t id = c + 32u * k + lane;
+          ok[k] = id < total;
+          x[k] = make_uint2(0, 0);
+          if (ok[k]) {
+            while (id >= nb) {
+              owner++;
+              nb = sstart[owner + 1];
+              bs = sbase[owner];
+            }
+            x[k] = __ldg(words + bs + id);
           }
-          x[k] = __ldg(prb_col + bs + id);
         }
-      }
 #pragma unroll
-      for (int k = 0; k < 4; k++) hits += ok[k] ? member<KIND>(bm, pv, x[k]) : 0u;
+        for (int k = 0; k < 4; k++) hits += ok[k] ? member_word<KIND>(bm, pv, x[k]) : 0u;
+      } else {
+        uint32_t x[4];
+        bool ok[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint32_t id = c + 32u * k + lane;
+          ok[k] = id < total;
+          x[k] = 0;
+          if (ok[k]) {
+            while (id >= nb) {
+              owner++;
+              nb = sstart[owner + 1];
+              bs = sbase[owner];
+            }
+            x[k] = __ldg(prb_col + bs + id);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) hits += ok[k] ? member<KIND>(bm, pv, x[k]) : 0u;
+      }
     }
     __syncwarp();
   }
@@ -187,7 +232,7 @@ __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, 
 // Build the pivot structure, probe entries [e, ee), restore the buffer to zero.
 // Split kind: ids >= base go to a bitmap of `words` words, the first `rlen`
 // ids of the row (those below base) to a sorted list after the zero word.
-template <uint32_t KIND, class Segs>
+template <uint32_t KIND, bool WORDS, class Segs>
 __device__ __forceinline__ uint32_t pivot_pass(const uint32_t* __restrict__ prow, uint32_t pd, uint32_t base,
                                                uint32_t words, uint32_t rlen, const Segs& segs, uint32_t e,
                                                uint32_t ee, const uint32_t* __restrict__ prb_col, uint32_t* bm,
@@ -221,7 +266,7 @@ __device__ __forceinline__ uint32_t pivot_pass(const uint32_t* __restrict__ prow
   pv.last = prow[pd - 1];
   pv.res = res;
   pv.rlen = rlen;
-  const uint32_t hits = probe_entries<KIND>(segs, e, ee, prb_col, bm, sstart, sbase, pv, lane);
+  const uint32_t hits = probe_entries<KIND, WORDS>(segs, e, ee, prb_col, bm, sstart, sbase, pv, lane);
   // the buffer is all-zero between pivots whatever kind used it last: the
   // persistent queue hands one warp bitmap and list work in any order
   __syncwarp();
@@ -290,14 +335,14 @@ __device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t
       const uint32_t* prow = p_col + ps;
       switch (tk.kind) {
         case kPivotBitmap:
-          acc += pivot_pass<kPivotBitmap>(prow, pd, 0, tk.words, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase,
+          acc += pivot_pass<kPivotBitmap, false>(prow, pd, 0, tk.words, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase,
                                           lane);
           break;
         case kPivotList:
-          acc += pivot_pass<kPivotList>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotList, false>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
           break;
         default:
-          acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotGlobal, false>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
       }
     }
     e = ee;
@@ -330,20 +375,25 @@ __device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_
       const uint32_t* prow = gi + ps;
       const uint32_t first = prow[0];
       const uint32_t last = prow[pd - 1];
-      const uint32_t span_words = ((last - first) >> 5) + 1;
+      // word-aligned bitmap: a streamed pair meets exactly one bitmap word
+      const uint32_t base = first & ~31u;
+      const uint32_t span_words = (last >> 5) - (first >> 5) + 1;
+      const uint32_t* gw = reinterpret_cast<const uint32_t*>(tk.g_words);
       if (span_words < bm_words) {
-        acc += pivot_pass<kPivotBitmap>(prow, pd, first, span_words, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+        acc += pivot_pass<kPivotBitmap, true>(prow, pd, base, span_words, 0, segs, e, ee, gw, bm, sstart, sbase,
+                                              lane);
       } else {
-        // bitmap over the top window of the row, the few ids below it in a short list
+        // bitmap over the top words of the row, the few ids below them in a short list
         const uint32_t wwords = bm_words - 1 - kSplitList;
-        const uint32_t wbase = last - (wwords * 32 - 1);
+        const uint32_t wbase = ((last >> 5) - (wwords - 1)) << 5;
         const uint32_t rlen = lower_bound_u32(prow, pd, wbase);
         if (rlen <= kSplitList)
-          acc += pivot_pass<kPivotSplit>(prow, pd, wbase, wwords, rlen, segs, e, ee, gi, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotSplit, true>(prow, pd, wbase, wwords, rlen, segs, e, ee, gw, bm, sstart, sbase,
+                                               lane);
         else if (pd <= bm_words)
-          acc += pivot_pass<kPivotList>(prow, pd, 0, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotList, true>(prow, pd, 0, 0, 0, segs, e, ee, gw, bm, sstart, sbase, lane);
         else
-          acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, 0, segs, e, ee, gi, bm, sstart, sbase, lane);
+          acc += pivot_pass<kPivotGlobal, true>(prow, pd, 0, 0, 0, segs, e, ee, gw, bm, sstart, sbase, lane);
       }
     }
     e = ee;
@@ -481,6 +531,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
           d.slot = (uint32_t)gi;
           d.g_indptr = g->d_indptr;
           d.g_indices = g->d_indices;
+          d.g_words = reinterpret_cast<const uint2*>(g->d_words);
           d.pivot_base = g->cuts[j];
           add(d, 0.5 * part_row_len(g, i));
         }
@@ -602,9 +653,10 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
         plan->cap = cap;
       }
       BBTC_CUDA(cudaMemcpyAsync(plan->d_tasks, plan->tasks.data(), nt * sizeof(DevTask), cudaMemcpyHostToDevice, s));
+      // pageable sources: the copies are staged before cudaMemcpyAsync returns,
+      // and plan->tasks / prefix live until the plan is rebuilt
       BBTC_CUDA(cudaMemcpyAsync(plan->d_prefix, plan->prefix.data(), (nt + 1) * sizeof(uint32_t),
                                 cudaMemcpyHostToDevice, s));
-      BBTC_CUDA(cudaStreamSynchronize(s));  // host staging buffers must outlive the copies
     }
     plan->captured = false;
   }
@@ -730,12 +782,12 @@ __global__ void __launch_bounds__(256, 4) k_count_csr_static(const uint32_t* __r
       const uint32_t first = prow[0], last = prow[pd - 1];
       const uint32_t span_words = last >= first ? ((last - first) >> 5) + 1 : 0xffffffffu;
       if (span_words < bm_words)
-        acc += pivot_pass<kPivotBitmap>(prow, pd, first, span_words, 0, segs, e, ee, indices, bm, sstart, sbase,
+        acc += pivot_pass<kPivotBitmap, false>(prow, pd, first, span_words, 0, segs, e, ee, indices, bm, sstart, sbase,
                                         lane);
       else if (pd <= bm_words)
-        acc += pivot_pass<kPivotList>(prow, pd, 0, 0, 0, segs, e, ee, indices, bm, sstart, sbase, lane);
+        acc += pivot_pass<kPivotList, false>(prow, pd, 0, 0, 0, segs, e, ee, indices, bm, sstart, sbase, lane);
       else
-        acc += pivot_pass<kPivotGlobal>(prow, pd, 0, 0, 0, segs, e, ee, indices, bm, sstart, sbase, lane);
+        acc += pivot_pass<kPivotGlobal, false>(prow, pd, 0, 0, 0, segs, e, ee, indices, bm, sstart, sbase, lane);
       e = ee;
       if (e < e1) u = next_row(indptr, n, u, e, lane);
     }

@@ -40,7 +40,7 @@ constexpr uint64_t kNoSegment = ~0ull;
 struct DevTile {
   const uint32_t* rp;
   const uint32_t* col;
-  const uint2* rec;  // reversed tiles: (e + 1, end of row u) of each entry's forward edge e = (u, v)
+  const uint2* rec;  // reversed tiles: pair range [word of v, end) in row u, per entry's forward edge (u, v)
   uint32_t H, W, nnz, maxdeg;
 };
 
@@ -65,6 +65,7 @@ struct DevTask {
   DevTile probe;
   const uint32_t* g_indptr;   // fused task rows: the resident oriented CSR
   const uint32_t* g_indices;
+  const uint2* g_words;       // fused: word-compressed rows
   uint32_t pivot_base;        // fused: first vertex id of part j
   uint32_t kind;
   uint32_t unit_edges;  // entries of `rows` per work unit
@@ -116,6 +117,8 @@ struct bbtc_graph {
   std::vector<uint32_t> cuts;
   uint32_t* d_indptr = nullptr;   // resident oriented CSR (global ids)
   uint32_t* d_indices = nullptr;
+  void* d_words = nullptr;        // word-compressed rows: (word, mask) uint2 pairs
+  uint32_t* d_wptr = nullptr;     // n + 1 pair offsets
   bbtc::BlockTiles fwd, rev;
   uint64_t* d_count = nullptr;  // result slot
   uint64_t device_bytes = 0;

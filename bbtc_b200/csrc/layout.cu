@@ -13,8 +13,11 @@
 //     the reference's tiles, used as ab / bc / ac by the per-task kernels;
 //   * reversed tiles (y, x): the same edges grouped by their column vertex --
 //     the CSC of forward tile (x, y) -- with, beside each entry, the record
-//     (e + 1, end of row u) of its forward edge e = (u, v): the ids of N+(u)
-//     that follow v, which is what a fused task row streams per entry.
+//     of its forward edge (u, v): the range of row u's word-compressed pairs
+//     from the one that holds v to the row's end, which is what a fused task
+//     row streams per entry;
+//   * the word-compressed rows of the oriented CSR: row u's ids grouped by
+//     32-id word into (word index, bit mask) pairs.
 //
 // Every tile owns a row-pointer segment of H+1 tile-local offsets (first
 // entry 0) in one pool, laid out like the reference's rows_ array (P segments
@@ -66,14 +69,16 @@ __global__ void k_validate_rows(const uint32_t* __restrict__ indptr, uint32_t n,
   }
 }
 
-// Needs valid row pointers: expands the row id of every edge and checks ids.
+// Expands the row id of every edge and checks ids; rows whose pointers are
+// out of order or past m are skipped (k_validate_rows flags them).
 __global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
-                               uint32_t n, uint32_t* __restrict__ rows, uint32_t* __restrict__ bad) {
+                               uint32_t n, uint64_t m, uint32_t* __restrict__ rows, uint32_t* __restrict__ bad) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = warp; u < n; u += nwarps) {
     const uint32_t a = indptr[u], b = indptr[u + 1];
+    if (b < a || (uint64_t)b > m) continue;
     for (uint32_t e = a + lane; e < b; e += 32) {
       rows[e] = u;
       const uint32_t c = indices[e];
@@ -194,8 +199,8 @@ __global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint3
                                 const uint32_t* __restrict__ rows, uint64_t m, const uint32_t* __restrict__ cuts_g,
                                 uint32_t P, const uint64_t* __restrict__ rp_off, const uint64_t* __restrict__ col_off,
                                 const uint32_t* __restrict__ rp, uint32_t* __restrict__ col,
-                                const uint32_t* __restrict__ eids, const uint32_t* __restrict__ fwd_indptr,
-                                uint2* __restrict__ rec) {
+                                const uint32_t* __restrict__ eids, const uint32_t* __restrict__ wpos,
+                                const uint32_t* __restrict__ wptr, uint2* __restrict__ rec) {
   __shared__ uint32_t cuts[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
   __syncthreads();
@@ -211,9 +216,48 @@ __global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint3
     const uint64_t pos = col_off[t] + rp[rp_off[t] + (u - cuts[x])] + ((uint32_t)e - run);
     col[pos] = c - cuts[y];
     if (rec) {
-      const uint32_t fe = eids[e];  // forward edge (c -> u) of this reversed entry
-      rec[pos] = make_uint2(fe + 1, fwd_indptr[c + 1]);
+      // forward edge fe = (c -> u) of this reversed entry: the pairs of row c
+      // from the one holding u to the row's end
+      const uint32_t fe = eids[e];
+      rec[pos] = make_uint2(wpos[fe], wptr[c + 1]);
     }
+  }
+}
+
+// Word-compressed rows: each row's ids grouped by 32-id word into (word, bit
+// mask) pairs.  flags[e] = 1 when edge e opens a new word of its row.
+__global__ void k_word_flags(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+                             const uint32_t* __restrict__ rows, uint64_t m, uint32_t* __restrict__ flags) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride)
+    flags[e] = (e == indptr[rows[e]] || (indices[e] >> 5) != (indices[e - 1] >> 5)) ? 1u : 0u;
+}
+
+// After an inclusive scan of the flags, wpos[e] - 1 is the pair edge e lands in
+// (k_word_index turns the scan into that index).
+__global__ void k_word_index(uint32_t* __restrict__ wpos, uint64_t m) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) wpos[e] -= 1;
+}
+
+// wpos[e]: the pair edge e lands in.
+__global__ void k_word_fill(const uint32_t* __restrict__ indices, const uint32_t* __restrict__ flags,
+                            const uint32_t* __restrict__ wpos, uint64_t m, uint2* __restrict__ words) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
+    const uint32_t x = indices[e];
+    const uint32_t p = wpos[e];
+    if (flags[e]) words[p].x = x >> 5;
+    atomicOr(&words[p].y, 1u << (x & 31));
+  }
+}
+
+// wptr[u] = first pair of row u (u in [0, n]); a row's first edge opens a pair.
+__global__ void k_word_rowptr(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ wpos, uint32_t n,
+                              uint64_t m, uint32_t* __restrict__ wptr) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= n; u += gridDim.x * blockDim.x) {
+    const uint32_t e = indptr[u];
+    wptr[u] = (uint64_t)e < m ? wpos[e] : (m ? wpos[m - 1] + 1 : 0u);
   }
 }
 
@@ -274,8 +318,8 @@ int dalloc(DevBuf& b, size_t bytes, cudaStream_t s) {
 // and are copied to the host by the caller.
 int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const uint32_t* d_indices,
                 const uint32_t* d_rows, uint32_t n, uint64_t m, const std::vector<uint32_t>& cuts,
-                const uint32_t* d_cuts, const uint32_t* eids, const uint32_t* fwd_indptr, uint32_t* d_stats,
-                uint64_t* d_coloff, int grid) {
+                const uint32_t* d_cuts, const uint32_t* eids, const uint32_t* wpos, const uint32_t* wptr,
+                uint32_t* d_stats, uint64_t* d_coloff, int grid) {
   const uint32_t P = (uint32_t)cuts.size() - 1;
   const uint32_t T = P * P;
   cudaStream_t s = ctx->stream;
@@ -336,22 +380,29 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   BBTC_CUDA(cudaGetLastError());
   if (m > 0) {
     k_entry_scatter<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
-                                         bt.d_col, eids, fwd_indptr, reinterpret_cast<uint2*>(bt.d_rec));
+                                         bt.d_col, eids, wpos, wptr, reinterpret_cast<uint2*>(bt.d_rec));
     BBTC_CUDA(cudaGetLastError());
   }
   return BBTC_OK;
 }
 
-int fetch_stats(BlockTiles& bt, const uint32_t* d_stats, const uint64_t* d_coloff, cudaStream_t s) {
-  const uint32_t T = bt.P * bt.P;
-  std::vector<uint32_t> h(3 * T);
-  BBTC_CUDA(cudaMemcpyAsync(h.data(), d_stats, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  bt.col_off.assign(T, kNoSegment);
-  BBTC_CUDA(cudaMemcpyAsync(bt.col_off.data(), d_coloff, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+int fetch_stats(BlockTiles& a, BlockTiles& b, const uint32_t* d_stats_a, const uint64_t* d_coloff_a,
+                const uint32_t* d_stats_b, const uint64_t* d_coloff_b, cudaStream_t s) {
+  const uint32_t T = a.P * a.P;
+  std::vector<uint32_t> ha(3 * T), hb(3 * T);
+  BBTC_CUDA(cudaMemcpyAsync(ha.data(), d_stats_a, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  BBTC_CUDA(cudaMemcpyAsync(hb.data(), d_stats_b, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  a.col_off.assign(T, kNoSegment);
+  b.col_off.assign(T, kNoSegment);
+  BBTC_CUDA(cudaMemcpyAsync(a.col_off.data(), d_coloff_a, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  BBTC_CUDA(cudaMemcpyAsync(b.col_off.data(), d_coloff_b, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   BBTC_CUDA(cudaStreamSynchronize(s));
-  bt.nnz.assign(h.begin(), h.begin() + T);
-  bt.maxdeg.assign(h.begin() + T, h.begin() + 2 * T);
-  bt.nerows.assign(h.begin() + 2 * T, h.end());
+  for (auto* p : {&a, &b}) {
+    const auto& h = p == &a ? ha : hb;
+    p->nnz.assign(h.begin(), h.begin() + T);
+    p->maxdeg.assign(h.begin() + T, h.begin() + 2 * T);
+    p->nerows.assign(h.begin() + 2 * T, h.end());
+  }
   return BBTC_OK;
 }
 
@@ -418,26 +469,25 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   const uint32_t* d_indptr = g->d_indptr;
   const uint32_t* d_indices = g->d_indices;
 
-  DevBuf d_cuts, bad, rows, stats, coloff;
+  DevBuf d_cuts, bad, rows, stats, coloff, stats_r, coloff_r;
   BBTC_TRY(dalloc(d_cuts, g->cuts.size() * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(bad, sizeof(uint32_t), s));
   BBTC_TRY(dalloc(rows, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(stats, 4 * T * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(coloff, T * sizeof(uint64_t), s));
+  BBTC_TRY(dalloc(stats_r, 4 * T * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(coloff_r, T * sizeof(uint64_t), s));
   BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, g->cuts.data(), g->cuts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
   uint32_t hbad = 0;
   if (n > 0) {
+    // both checks, one read-back: nothing indexes by the input before it passes
     k_validate_rows<<<grid, 256, 0, s>>>(d_indptr, n, m, bad.as<uint32_t>());
+    BBTC_CUDA(cudaGetLastError());
+    k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>());
     BBTC_CUDA(cudaGetLastError());
     BBTC_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     BBTC_CUDA(cudaStreamSynchronize(s));
-    if (!hbad) {
-      k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, rows.as<uint32_t>(), bad.as<uint32_t>());
-      BBTC_CUDA(cudaGetLastError());
-      BBTC_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-      BBTC_CUDA(cudaStreamSynchronize(s));
-    }
   }
   if (hbad) {
     std::string why;
@@ -450,8 +500,37 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   }
 
   BBTC_TRY(build_block(ctx, g->fwd, d_indptr, d_indices, rows.as<uint32_t>(), n, m, g->cuts, d_cuts.as<uint32_t>(),
-                       nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
-  BBTC_TRY(fetch_stats(g->fwd, stats.as<uint32_t>(), coloff.as<uint64_t>(), s));
+                       nullptr, nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
+
+  // word-compressed rows (the fused task rows stream these)
+  DevBuf wflags, wpos;
+  BBTC_TRY(dalloc(wflags, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(wpos, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+  {
+    cudaError_t e1 = cudaMallocAsync(&g->d_words, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s);
+    cudaError_t e2 = cudaMallocAsync(&g->d_wptr, ((size_t)n + 1) * sizeof(uint32_t), s);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+      cudaGetLastError();
+      return fail(BBTC_ERR_NOMEM, "device allocation of the word-compressed rows failed");
+    }
+    BBTC_CUDA(cudaMemsetAsync(g->d_words, 0, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s));
+    if (m > 0) {
+      k_word_flags<<<grid, 256, 0, s>>>(d_indptr, d_indices, rows.as<uint32_t>(), m, wflags.as<uint32_t>());
+      BBTC_CUDA(cudaGetLastError());
+      size_t tb = 0;
+      BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, wflags.as<uint32_t>(), wpos.as<uint32_t>(), (int64_t)m, s));
+      DevBuf tmp;
+      BBTC_TRY(dalloc(tmp, tb, s));
+      BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, wflags.as<uint32_t>(), wpos.as<uint32_t>(), (int64_t)m, s));
+      k_word_index<<<grid, 256, 0, s>>>(wpos.as<uint32_t>(), m);
+      BBTC_CUDA(cudaGetLastError());
+      k_word_fill<<<grid, 256, 0, s>>>(d_indices, wflags.as<uint32_t>(), wpos.as<uint32_t>(), m,
+                                       reinterpret_cast<uint2*>(g->d_words));
+      BBTC_CUDA(cudaGetLastError());
+    }
+    k_word_rowptr<<<grid, 256, 0, s>>>(d_indptr, wpos.as<uint32_t>(), n, m, g->d_wptr);
+    BBTC_CUDA(cudaGetLastError());
+  }
 
   // reversed graph: a stable sort of (column, forward edge id) by column keeps
   // every in-list ordered by source
@@ -483,17 +562,20 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     BBTC_CUDA(cudaGetLastError());
     // reversed entries: row = column vertex v (keys), column = source u, record of forward edge (u, v)
     BBTC_TRY(build_block(ctx, g->rev, rev_indptr.as<uint32_t>(), rev_cols.as<uint32_t>(), keys_out.as<uint32_t>(),
-                         n, m, g->cuts, d_cuts.as<uint32_t>(), eids_out.as<uint32_t>(), d_indptr,
-                         stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
-    BBTC_TRY(fetch_stats(g->rev, stats.as<uint32_t>(), coloff.as<uint64_t>(), s));
+                         n, m, g->cuts, d_cuts.as<uint32_t>(), eids_out.as<uint32_t>(), wpos.as<uint32_t>(),
+                         g->d_wptr, stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), grid));
   }
+  // the host needs the tile statistics only now: one read-back for both block CSRs
+  BBTC_TRY(fetch_stats(g->fwd, g->rev, stats.as<uint32_t>(), coloff.as<uint64_t>(), stats_r.as<uint32_t>(),
+                       coloff_r.as<uint64_t>(), s));
   BBTC_CUDA(cudaEventRecord(ev1, s));
   BBTC_CUDA(cudaEventSynchronize(ev1));
   float ms = 0;
   BBTC_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   g->layout_ms = ms;
   g->device_bytes = (g->fwd.rp_len + g->fwd.col_len + g->rev.rp_len + g->rev.col_len) * sizeof(uint32_t) +
-                    g->rev.col_len * sizeof(uint2) + ((uint64_t)n + 1 + m) * sizeof(uint32_t) + 64 * sizeof(uint64_t);
+                    g->rev.col_len * sizeof(uint2) + ((uint64_t)n + 1 + m) * sizeof(uint32_t) + 64 * sizeof(uint64_t) +
+                    m * sizeof(uint2) + ((uint64_t)n + 1) * sizeof(uint32_t);
   return BBTC_OK;
 }
 

@@ -64,7 +64,7 @@ struct Request {
   int status = 0;  // 0 pending, 1 loading, 2 ready, 3 running, 4 done, < 0 failed
   uint64_t count = 0;
   uint32_t batch = 0;
-  uint64_t t_submit = 0, t_done = 0;
+  uint64_t t_submit = 0, t_done = 0, t_load = 0, t_ready = 0, t_launch = 0;
 };
 
 }  // namespace
@@ -119,6 +119,7 @@ void loader_main(bbtc_server* s, bbtc_ctx* ctx) {
     }
     s->in_use += r->reserved;
     r->status = 1;
+    r->t_load = now_ns();
     s->loading++;
     lk.unlock();
     bbtc_graph* g = nullptr;
@@ -140,6 +141,7 @@ void loader_main(bbtc_server* s, bbtc_ctx* ctx) {
     r->reserved = g->device_bytes;
     r->g = g;
     r->status = 2;
+    r->t_ready = now_ns();
     s->ready.push_back(r);
     s->cv_run.notify_one();
     s->cv_load.notify_all();
@@ -159,7 +161,11 @@ void launcher_main(bbtc_server* s) {
       batch.push_back(s->ready.front());
       s->ready.pop_front();
     }
-    for (Request* r : batch) r->status = 3;
+    const uint64_t t_launch = now_ns();
+    for (Request* r : batch) {
+      r->status = 3;
+      r->t_launch = t_launch;
+    }
     lk.unlock();
     std::vector<bbtc_graph*> gs;
     std::vector<std::vector<bbtc_task>> tl(batch.size());
@@ -185,8 +191,8 @@ void launcher_main(bbtc_server* s) {
       if (e2 != cudaSuccess) rc = cuda_fail(e2, "server batch readback");
     }
     const uint64_t t = now_ns();
+    // stream-ordered frees: the memory returns to the pool behind this launch
     for (Request* r : batch) graph_release_on(r->g, ctx->stream);
-    cudaStreamSynchronize(ctx->stream);
     lk.lock();
     for (size_t i = 0; i < batch.size(); i++) {
       Request* r = batch[i];
@@ -218,6 +224,9 @@ void fill_info(const Request* r, bbtc_request_info* info) {
   info->batch = r->batch;
   info->submit_ns = r->t_submit;
   info->done_ns = r->t_done;
+  info->load_ns = r->t_load;
+  info->ready_ns = r->t_ready;
+  info->launch_ns = r->t_launch;
 }
 
 }  // namespace

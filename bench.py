@@ -287,6 +287,7 @@ def run_serve(args):
     th = threading.Thread(target=submitter)
     th.start()
     lat, lat18, edges, first_sub, last_done = [], [], 0, None, 0
+    stages = {"queue": [], "load": [], "ready_wait": [], "count": []}
     for i in range(n_req):
         while ids[i] is None:
             time.sleep(0.0002)
@@ -294,6 +295,10 @@ def run_serve(args):
         assert info.status == 1
         ms = (info.done_ns - info.submit_ns) / 1e6
         lat.append(ms)
+        stages["queue"].append((info.load_ns - info.submit_ns) / 1e6)
+        stages["load"].append((info.ready_ns - info.load_ns) / 1e6)
+        stages["ready_wait"].append((info.launch_ns - info.ready_ns) / 1e6)
+        stages["count"].append((info.done_ns - info.launch_ns) / 1e6)
         if scales[i] <= 18:
             lat18.append(ms)
         edges += picks[i][0].m
@@ -313,7 +318,9 @@ def run_serve(args):
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "p50_scale_le_18": float(np.percentile(lat18, 50)) if lat18 else None,
                           "p99_scale_le_18": float(np.percentile(lat18, 99)) if lat18 else None,
-                          "definition": "bbtc_submit -> count in host memory (server steady clock)"}}
+                          "definition": "bbtc_submit -> count in host memory (server steady clock)"},
+           "stages_ms_p50_p99": {k: [float(np.percentile(v, 50)), float(np.percentile(v, 99))]
+                                 for k, v in stages.items()}}
     print(json.dumps(res), flush=True)
 
 
@@ -328,8 +335,11 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
     if world > 1:
-        import torch.distributed as dist
         import datetime
+        import torch
+        import torch.distributed as dist
+        if args.impl == "ours":
+            torch.cuda.set_device(local)  # before the NCCL communicator exists
         dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
                                 timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":

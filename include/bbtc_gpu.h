@@ -235,6 +235,9 @@ typedef struct bbtc_request_info {
   uint32_t batch;     /* graphs in the launch that counted it */
   uint64_t submit_ns; /* steady-clock time of bbtc_submit */
   uint64_t done_ns;   /* steady-clock time the count reached host memory */
+  uint64_t load_ns;   /* a loader took the request (upload + layout start) */
+  uint64_t ready_ns;  /* its layout was built */
+  uint64_t launch_ns; /* the launch that counted it was issued */
 } bbtc_request_info;
 typedef struct bbtc_server_stats {
   uint64_t launches, counted, max_batch, pending, ready, device_bytes_in_use;

@@ -146,6 +146,45 @@ def ref_cli(n: int, indptr, indices, partitioner: str = "pal", ncut: int = 8, nt
     return fields
 
 
+def write_bbtc(path: str, n: int, indptr, indices) -> None:
+    """The oriented CSR as a PIGO-CSR-v2 `.bbtc` file, the reference's cache
+    format (include/utils/utils.hpp:260-268), which it loads as the oriented
+    graph without re-reading text."""
+    indptr = np.ascontiguousarray(indptr, dtype=np.uint32)
+    indices = np.ascontiguousarray(indices, dtype=np.uint32)
+    with open(path, "wb") as f:
+        f.write(b"PIGO-CSR-v2")
+        f.write(bytes([4, 4]))
+        f.write(np.array([n, len(indices), n, n], dtype=np.uint32).tobytes())
+        f.write(indptr.tobytes())
+        f.write(indices.tobytes())
+
+
+def ref_gpu_cli(n: int, indptr, indices, partitioner: str = "pal", ncut: int = 16, repeat: int = 5,
+                timeout: int = 900) -> dict:
+    """The reference's unmodified CUDA executable (oracle/_ref/bbtc_gpu):
+    `--ngpu 1 --border -1 --copy-first`, its one-launch-per-task GPU form.
+    Returns the count and its "Triangle Counting Execution Time (s)" lines."""
+    exe = os.path.join(HERE, "_ref", "bbtc_gpu")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "g.bbtc")
+        write_bbtc(path, n, indptr, indices)
+        res = subprocess.run([exe, "--graph", path, "--partitioner", partitioner, "--ncut", str(ncut), "--ngpu", "1",
+                              "--border", "-1", "--copy-first", "--repeat", str(repeat)],
+                             capture_output=True, text=True, timeout=timeout)
+    out = res.stdout
+    m = re.search(r"Number of Triangles: (\d+)", out)
+    if not m:
+        raise RuntimeError(f"reference GPU executable failed:\n{out}\n{res.stderr}")
+    times = [float(x) for x in re.findall(r"Triangle Counting Execution Time \(s\) : ([0-9.]+)", out)]
+    copy = [float(x) for x in re.findall(r"Copy tiles to device \(s\) : ([0-9.]+)", out)]
+    layout = re.search(r"Partitioning and Layout construction \(s\) : ([0-9.]+)", out)
+    return {"triangles": int(m.group(1)), "count_seconds": times, "copy_seconds": copy,
+            "layout_seconds": float(layout.group(1)) if layout else None, "stdout": out}
+
+
 def brute_force(n: int, indptr, indices) -> int:
     """Triangles of the undirected graph the CSR represents, by checking every
     vertex triple (tiny graphs only)."""
