@@ -22,7 +22,8 @@ class TuneSpace(ctypes.Structure):
     _fields_ = [("bitmap_words", ctypes.POINTER(ctypes.c_uint32)), ("n_bitmap_words", ctypes.c_uint32),
                 ("warps_per_block", ctypes.POINTER(ctypes.c_uint32)), ("n_warps_per_block", ctypes.c_uint32),
                 ("unit_work", ctypes.POINTER(ctypes.c_uint32)), ("n_unit_work", ctypes.c_uint32),
-                ("repeats", ctypes.c_uint32)]
+                ("repeats", ctypes.c_uint32), ("occupancy", ctypes.POINTER(ctypes.c_uint32)),
+                ("n_occupancy", ctypes.c_uint32)]
 
 
 def cache_path() -> str:
@@ -52,7 +53,7 @@ def _arr(vals):
 
 
 def sweep(graph: core.Graph, base: core.Opts | None = None, bitmap_words=None, warps_per_block=None,
-          unit_work=None, repeats: int = 3) -> tuple[core.Opts, float]:
+          unit_work=None, occupancy=None, repeats: int = 3) -> tuple[core.Opts, float]:
     """Run the library's sweep; returns the fastest options and their median ms."""
     lib = core.lib()
     lib.bbtc_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(TuneSpace),
@@ -66,7 +67,7 @@ def sweep(graph: core.Graph, base: core.Opts | None = None, bitmap_words=None, w
     sp = TuneSpace()
     keep = []
     for field, vals in (("bitmap_words", bitmap_words), ("warps_per_block", warps_per_block),
-                        ("unit_work", unit_work)):
+                        ("unit_work", unit_work), ("occupancy", occupancy)):
         if vals:
             arr, n = _arr(list(vals))
             keep.append(arr)

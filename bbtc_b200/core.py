@@ -46,7 +46,7 @@ class Task(c.Structure):
 class Opts(c.Structure):
     _fields_ = [("mode", c.c_int), ("kernel", c.c_int), ("bitmap_words", c.c_uint32),
                 ("warps_per_block", c.c_uint32), ("unit_work", c.c_uint32), ("blocks_per_sm", c.c_uint32),
-                ("use_cuda_graph", c.c_int), ("sort_tasks", c.c_int)]
+                ("use_cuda_graph", c.c_int), ("sort_tasks", c.c_int), ("occupancy", c.c_uint32)]
 
 
 class GraphInfo(c.Structure):
@@ -108,7 +108,7 @@ def check(rc: int) -> None:
 
 def options(mode: str | int = "persistent", kernel: str | int = "auto", bitmap_words: int = 0,
             warps_per_block: int = 0, unit_work: int = 0, blocks_per_sm: int = 0, cuda_graph: bool = True,
-            sort_tasks: bool = True) -> Opts:
+            sort_tasks: bool = True, occupancy: int = 0) -> Opts:
     o = Opts()
     lib().bbtc_opts_default(c.byref(o))
     o.mode = MODES[mode] if isinstance(mode, str) else int(mode)
@@ -122,6 +122,8 @@ def options(mode: str | int = "persistent", kernel: str | int = "auto", bitmap_w
     o.blocks_per_sm = blocks_per_sm
     o.use_cuda_graph = 1 if cuda_graph else 0
     o.sort_tasks = 1 if sort_tasks else 0
+    if occupancy:
+        o.occupancy = occupancy
     return o
 
 

@@ -304,10 +304,11 @@ void bbtc_opts_default(bbtc_opts* o) {
   o->kernel = BBTC_KERNEL_AUTO;
   o->bitmap_words = 1024;
   o->warps_per_block = 8;
-  o->unit_work = 8192;
+  o->unit_work = 0;
   o->blocks_per_sm = 0;
   o->use_cuda_graph = 1;
   o->sort_tasks = 1;
+  o->occupancy = 6;
 }
 
 static int count_async_impl(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint32_t ntasks, int32_t border,
@@ -379,10 +380,12 @@ int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bb
   if (!ctx || !g || !inout) return fail(BBTC_ERR_ARG, "NULL argument");
   static const uint32_t kWords[] = {256, 512, 1024, 2048, 4096};
   static const uint32_t kWarps[] = {4, 8};
-  static const uint32_t kWork[] = {2048, 8192, 32768};
-  bbtc_tune_space sp{kWords, 5, kWarps, 2, kWork, 3, 3};
+  static const uint32_t kWork[] = {256, 2048, 8192};
+  static const uint32_t kOcc[] = {4, 6, 8};
+  bbtc_tune_space sp{kWords, 5, kWarps, 2, kWork, 3, 3, kOcc, 3};
   if (space) {
     sp = *space;
+    if (!sp.occupancy || !sp.n_occupancy) { sp.occupancy = kOcc; sp.n_occupancy = 3; }
     if (!sp.bitmap_words || !sp.n_bitmap_words) { sp.bitmap_words = kWords; sp.n_bitmap_words = 5; }
     if (!sp.warps_per_block || !sp.n_warps_per_block) { sp.warps_per_block = kWarps; sp.n_warps_per_block = 2; }
     if (!sp.unit_work || !sp.n_unit_work) { sp.unit_work = kWork; sp.n_unit_work = 3; }
@@ -402,11 +405,13 @@ int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bb
   bool have_ref = false;
   for (uint32_t iw = 0; iw < sp.n_bitmap_words; iw++)
     for (uint32_t ip = 0; ip < sp.n_warps_per_block; ip++)
-      for (uint32_t iu = 0; iu < sp.n_unit_work; iu++) {
+      for (uint32_t iu = 0; iu < sp.n_unit_work; iu++)
+      for (uint32_t io = 0; io < sp.n_occupancy; io++) {
         bbtc_opts o = *inout;
         o.bitmap_words = sp.bitmap_words[iw];
         o.warps_per_block = sp.warps_per_block[ip];
         o.unit_work = sp.unit_work[iu];
+        o.occupancy = sp.occupancy[io];
         if (smem_bytes_for(o) > ctx->smem_optin) continue;  // does not fit this device
         uint64_t c = 0;
         BBTC_TRY(bbtc_count(ctx, g, nullptr, 0, -1, &o, &c));  // warm-up, builds the plan

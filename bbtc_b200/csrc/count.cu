@@ -47,7 +47,10 @@ namespace bbtc {
 namespace {
 
 constexpr uint32_t FULL = 0xffffffffu;
-constexpr uint32_t kSegWords = 72;  // per-warp: 33 segment starts + 32 bases (+ pad)
+// per warp after its bitmap: 33 segment starts, 32 bases, a pad word and the
+// 8-byte aligned FusedFrame (22 words), rounded up to an even count
+constexpr uint32_t kSegWords = 96;
+constexpr uint32_t kFrameOffset = 66;  // words after the bitmap
 constexpr uint32_t kSplitList = 128; // split pivots: room for the ids below the bitmap window
 
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t x) {
@@ -325,7 +328,7 @@ __device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t
   const uint64_t e1w = e0 + tk.unit_edges;
   uint32_t e = (uint32_t)e0;
   const uint32_t e1 = e1w < tk.rows.nnz ? (uint32_t)e1w : tk.rows.nnz;
-  uint32_t b = row_of(r_rp, H, e);
+  uint32_t b = tk.rows.erow[e >> 5];  // units start at multiples of 32 entries
   unsigned long long acc = 0;
   while (e < e1) {
     const uint32_t ee = min(r_rp[b + 1], e1);
@@ -364,7 +367,7 @@ __device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_
   const uint64_t e1w = e0 + tk.unit_edges;
   uint32_t e = (uint32_t)e0;
   const uint32_t e1 = e1w < tk.rows.nnz ? (uint32_t)e1w : tk.rows.nnz;
-  uint32_t b = row_of(r_rp, H, e);
+  uint32_t b = tk.rows.erow[e >> 5];  // units start at multiples of 32 entries
   unsigned long long acc = 0;
   while (e < e1) {
     const uint32_t ee = min(r_rp[b + 1], e1);
@@ -415,8 +418,10 @@ __device__ __forceinline__ unsigned long long dispatch_unit(const DevTask& tk, u
   return task_unit(tk, unit, bm, sstart, sbase, lane);
 }
 
-// Persistent form: every warp claims units from one head until the queue is empty.
-__global__ void __launch_bounds__(256, 4) k_count_queue(const DevTask* __restrict__ tasks,
+// Persistent form: every warp claims units from one head until the queue is
+// empty.  MINB is the register budget's occupancy target (blocks per SM).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_count_queue(const DevTask* __restrict__ tasks,
                                                         const uint32_t* __restrict__ prefix, uint32_t ntasks,
                                                         uint32_t total_units, uint32_t* __restrict__ head,
                                                         unsigned long long* __restrict__ outs, uint32_t bm_words) {
@@ -462,6 +467,248 @@ __global__ void __launch_bounds__(256, 4) k_count_task(const DevTask* __restrict
   if (lane == 0 && acc) atomicAdd(&outs[tk.slot], acc);
 }
 
+// Fused persistent form.  A unit's loop state lives in a per-warp frame in
+// shared memory while the probe loop runs, so the loop keeps the whole
+// register budget (the persistent kernel runs at 40 registers per thread to
+// keep 48 warps per SM resident; state held in registers across the probe
+// loop would spill to local memory, which misses the small L1 left beside
+// the bitmaps).  Lane 0 writes the frame; every lane reads it back after a
+// __syncwarp.
+struct FusedFrame {
+  const uint32_t* rp;    // reversed tile (j, i): row pointers
+  const uint2* rec;      // its forward-edge records
+  const uint32_t* gp;    // oriented CSR
+  const uint32_t* gi;
+  const uint2* gw;       // word-compressed rows
+  uint32_t H, e1, b, ee; // rows, unit end, current row, end of the current row's entries
+  uint32_t pivot_base, ps, pd, base, words, rlen, kind, slot;
+};
+static_assert(sizeof(FusedFrame) <= (kSegWords - kFrameOffset) * sizeof(uint32_t), "frame does not fit");
+
+enum : uint32_t { kNoPivot = 0xffffffffu };
+
+// Choose the pivot structure of row v (ids prow[0..pd)) and record it in the frame.
+__device__ __forceinline__ void fused_choose(volatile FusedFrame* fr, const uint32_t* __restrict__ prow, uint32_t pd,
+                                             uint32_t bm_words, uint32_t lane) {
+  uint32_t kind = kNoPivot, base = 0, words = 0, rlen = 0;
+  if (pd > 0) {
+    const uint32_t first = prow[0];
+    const uint32_t last = prow[pd - 1];
+    const uint32_t span_words = (last >> 5) - (first >> 5) + 1;
+    if (span_words < bm_words) {
+      kind = kPivotBitmap;
+      base = first & ~31u;  // word-aligned: a streamed pair meets exactly one bitmap word
+      words = span_words;
+    } else {
+      // bitmap over the top words of the row, the few ids below them in a short list
+      const uint32_t wwords = bm_words - 1 - kSplitList;
+      const uint32_t wbase = ((last >> 5) - (wwords - 1)) << 5;
+      rlen = lower_bound_u32(prow, pd, wbase);
+      if (rlen <= kSplitList) {
+        kind = kPivotSplit;
+        base = wbase;
+        words = wwords;
+      } else {
+        kind = pd <= bm_words ? kPivotList : kPivotGlobal;
+        rlen = 0;
+      }
+    }
+  }
+  if (lane == 0) {
+    fr->pd = pd;
+    fr->kind = kind;
+    fr->base = base;
+    fr->words = words;
+    fr->rlen = rlen;
+  }
+}
+
+template <uint32_t KIND>
+__device__ __forceinline__ void fused_build(const uint32_t* __restrict__ prow, uint32_t pd, uint32_t base,
+                                            uint32_t rlen, uint32_t* bm, uint32_t* res, uint32_t lane) {
+  if constexpr (KIND == kPivotBitmap) {
+    for (uint32_t i = lane; i < pd; i += 32) {
+      const uint32_t y = prow[i] - base;
+      atomicOr(&bm[y >> 5], 1u << (y & 31));
+    }
+  } else if constexpr (KIND == kPivotSplit) {
+    for (uint32_t i = lane; i < pd; i += 32) {
+      const uint32_t x = prow[i];
+      if (i < rlen) {
+        res[i] = x;
+      } else {
+        const uint32_t y = x - base;
+        atomicOr(&bm[y >> 5], 1u << (y & 31));
+      }
+    }
+  } else if constexpr (KIND == kPivotList) {
+    for (uint32_t i = lane; i < pd; i += 32) bm[i] = prow[i];
+  }
+}
+
+template <uint32_t KIND>
+__device__ __forceinline__ void fused_clear(const uint32_t* __restrict__ prow, uint32_t pd, uint32_t base,
+                                            uint32_t words, uint32_t rlen, uint32_t* bm, uint32_t* res,
+                                            uint32_t lane) {
+  // up to 512 words are cleared as a range (16 stores a lane, no loads);
+  // beyond that, the words of the row's ids, read again
+  if constexpr (KIND == kPivotBitmap) {
+    if (words <= 512 || pd >= words) {
+      for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
+    } else {
+      for (uint32_t i = lane; i < pd; i += 32) bm[(prow[i] - base) >> 5] = 0;
+    }
+  } else if constexpr (KIND == kPivotSplit) {
+    if (pd - rlen >= words) {
+      for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
+    } else {
+      for (uint32_t i = lane + rlen; i < pd; i += 32) bm[(prow[i] - base) >> 5] = 0;
+    }
+    for (uint32_t i = lane; i < rlen; i += 32) res[i] = 0;
+  } else if constexpr (KIND == kPivotList) {
+    for (uint32_t i = lane; i < pd; i += 32) bm[i] = 0;
+  }
+}
+
+// Probe entries [e, ee) of the frame's rows tile against the built pivot of kind KIND.
+template <uint32_t KIND>
+__device__ __forceinline__ uint32_t fused_probe(volatile FusedFrame* fr, const uint32_t* __restrict__ prow,
+                                                uint32_t e, uint32_t ee, uint32_t* bm, uint32_t* sstart,
+                                                uint32_t* sbase, uint32_t bm_words, uint32_t lane) {
+  PivotView pv;
+  pv.row = prow;
+  pv.len = fr->pd;
+  pv.base = fr->base;
+  pv.cap = fr->words * 32;
+  pv.first = KIND == kPivotBitmap ? 0u : prow[0];
+  pv.last = KIND == kPivotBitmap ? 0u : prow[pv.len - 1];
+  pv.res = bm + fr->words + 1;
+  pv.rlen = fr->rlen;
+  const RecSegs segs{(const uint2*)fr->rec};
+  return probe_entries<KIND, true>(segs, e, ee, reinterpret_cast<const uint32_t*>(fr->gw), bm, sstart, sbase, pv,
+                                   lane);
+}
+
+// Pivots too wide for a span bitmap (split, list, global kinds): a separate
+// function, so their register needs do not weigh on the common bitmap path.
+__device__ __noinline__ uint32_t fused_wide(volatile FusedFrame* fr, uint32_t kind, const uint32_t* prow, uint32_t e,
+                                            uint32_t ee, uint32_t* bm, uint32_t* sstart, uint32_t* sbase,
+                                            uint32_t bm_words, uint32_t lane) {
+  uint32_t* res = bm + fr->words + 1;
+  if (kind == kPivotSplit) {
+    fused_build<kPivotSplit>(prow, fr->pd, fr->base, fr->rlen, bm, res, lane);
+    __syncwarp();
+    return fused_probe<kPivotSplit>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
+  }
+  if (kind == kPivotList) {
+    fused_build<kPivotList>(prow, fr->pd, 0, 0, bm, res, lane);
+    __syncwarp();
+    return fused_probe<kPivotList>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
+  }
+  __syncwarp();
+  return fused_probe<kPivotGlobal>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __restrict__ tasks,
+                                                        const uint32_t* __restrict__ prefix, uint32_t ntasks,
+                                                        uint32_t total_units, uint32_t* __restrict__ head,
+                                                        unsigned long long* __restrict__ outs, uint32_t bm_words) {
+  extern __shared__ __align__(16) uint32_t sh[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* bm = sh + warp * (bm_words + kSegWords);
+  uint32_t* sstart = bm + bm_words;
+  uint32_t* sbase = sstart + 33;
+  volatile FusedFrame* fr = reinterpret_cast<volatile FusedFrame*>(bm + bm_words + kFrameOffset);
+  for (uint32_t i = lane; i < bm_words; i += 32) bm[i] = 0;
+  __syncwarp();
+  while (true) {
+    uint32_t g = 0;
+    if (lane == 0) g = atomicAdd(head, 1u);
+    g = __shfl_sync(FULL, g, 0);
+    if (g >= total_units) break;
+    uint32_t lo = 0, hi = ntasks;  // last t with prefix[t] <= g
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (prefix[mid] <= g) lo = mid; else hi = mid;
+    }
+    if (lane == 0) {
+      const DevTask* tk = tasks + lo;
+      const uint32_t e0 = (g - prefix[lo]) * tk->unit_edges;  // < nnz < 2^32
+      const uint32_t nnz = tk->rows.nnz;
+      fr->rp = tk->rows.rp;
+      fr->rec = tk->rows.rec;
+      fr->gp = tk->g_indptr;
+      fr->gi = tk->g_indices;
+      fr->gw = tk->g_words;
+      fr->H = tk->rows.H;
+      fr->e1 = nnz - e0 > tk->unit_edges ? e0 + tk->unit_edges : nnz;
+      fr->b = tk->rows.erow[e0 >> 5];  // units start at multiples of 32 entries
+      fr->ee = e0;
+      fr->pivot_base = tk->pivot_base;
+      fr->slot = tk->slot;
+    }
+    __syncwarp();
+    unsigned long long acc = 0;
+    while (true) {
+      const uint32_t e = fr->ee;
+      if (e >= fr->e1) break;
+      // row b's entries in this unit and its pivot row N+(v), v = pivot_base + b
+      {
+        const uint32_t b = fr->b;
+        const uint32_t ee = min(fr->rp[b + 1], fr->e1);
+        const uint32_t v = fr->pivot_base + b;
+        const uint32_t ps = fr->gp[v];
+        const uint32_t pd = fr->gp[v + 1] - ps;
+        fused_choose(fr, fr->gi + ps, pd, bm_words, lane);
+        if (lane == 0) {
+          fr->ee = ee;
+          fr->ps = ps;
+        }
+        __syncwarp();
+      }
+      const uint32_t kind = fr->kind;
+      if (kind != kNoPivot) {
+        const uint32_t* prow = fr->gi + fr->ps;
+        const uint32_t ee = fr->ee;
+        uint32_t* res = bm + fr->words + 1;
+        switch (kind) {
+          case kPivotBitmap:
+            fused_build<kPivotBitmap>(prow, fr->pd, fr->base, 0, bm, res, lane);
+            __syncwarp();
+            acc += fused_probe<kPivotBitmap>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
+            break;
+          default:
+            acc += fused_wide(fr, kind, prow, e, ee, bm, sstart, sbase, bm_words, lane);
+        }
+        __syncwarp();
+        // the buffer returns to all-zero for the next pivot, whatever its kind
+        {
+          const uint32_t* prow2 = fr->gi + fr->ps;
+          uint32_t* res2 = bm + fr->words + 1;
+          switch (fr->kind) {
+            case kPivotBitmap: fused_clear<kPivotBitmap>(prow2, fr->pd, fr->base, fr->words, 0, bm, res2, lane); break;
+            case kPivotSplit:
+              fused_clear<kPivotSplit>(prow2, fr->pd, fr->base, fr->words, fr->rlen, bm, res2, lane);
+              break;
+            case kPivotList: fused_clear<kPivotList>(prow2, fr->pd, 0, 0, 0, bm, res2, lane); break;
+            default: break;
+          }
+        }
+        __syncwarp();
+      }
+      const uint32_t e2 = fr->ee;
+      if (e2 < fr->e1) {
+        const uint32_t nb = next_row(fr->rp, fr->H, fr->b, e2, lane);
+        if (lane == 0) fr->b = nb;
+      }
+      __syncwarp();
+    }
+    const unsigned long long c = warp_sum(acc);
+    if (lane == 0 && c) atomicAdd(&outs[fr->slot], c);
+  }
+}
+
 size_t smem_bytes(uint32_t bm_words, uint32_t warps) {
   return (size_t)warps * (bm_words + kSegWords) * sizeof(uint32_t);
 }
@@ -485,7 +732,12 @@ int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o) {
   if (sm > ctx->smem_optin)
     return fail(BBTC_ERR_ARG, "bitmap_words x warps_per_block needs " + std::to_string(sm) +
                                   " bytes of shared memory; the device allows " + std::to_string(ctx->smem_optin));
-  BBTC_CUDA(cudaFuncSetAttribute(k_count_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  BBTC_CUDA(cudaFuncSetAttribute(k_count_queue<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  BBTC_CUDA(cudaFuncSetAttribute(k_count_queue<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  BBTC_CUDA(cudaFuncSetAttribute(k_count_queue<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_count_task, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   return BBTC_OK;
 }
@@ -508,7 +760,9 @@ static double part_row_len(const bbtc_graph* g, uint32_t i) {
 static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<std::vector<bbtc_task>>& tasks,
                      const bbtc_opts& o, bool fused, Plan* plan) {
   const uint32_t bmw = norm_bm_words(o.bitmap_words);
-  const uint32_t unit_work = o.unit_work ? o.unit_work : 8192;
+  // default unit size: task rows of the fused form run best as 32-entry
+  // units (the floor below); explicit task lists as units of ~8192 probes
+  const uint32_t unit_work = o.unit_work ? o.unit_work : (fused ? 256 : 8192);
   std::vector<DevTask> list;
   std::vector<double> cost;
   auto add = [&](DevTask d, double avg_probe) {
@@ -583,6 +837,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
     plan->prefix.push_back((uint32_t)total);
   }
   plan->total_units = (uint32_t)total;
+  plan->fused = fused;
   return BBTC_OK;
 }
 
@@ -615,14 +870,18 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
       plan->launches++;
     }
   } else {
+    // the register budget: 4, 6 (default) or 8 resident blocks per SM
+    const uint32_t occ = o.occupancy >= 8 ? 8 : (o.occupancy >= 6 ? 6 : 4);
+    auto* kern = plan->fused ? (occ == 8 ? k_fused_queue<8> : (occ == 6 ? k_fused_queue<6> : k_fused_queue<4>))
+                             : (occ == 8 ? k_count_queue<8> : (occ == 6 ? k_count_queue<6> : k_count_queue<4>));
     int per_sm = 0;
-    BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count_queue, wpb * 32, sm));
+    BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, sm));
     per_sm = std::max(1, per_sm);
     if (o.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)o.blocks_per_sm);
     const uint32_t grid = ctx->sms * per_sm;
     BBTC_CUDA(cudaMemsetAsync(ctx->d_unit_counter, 0, sizeof(uint32_t), s));
-    k_count_queue<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units,
-                                             ctx->d_unit_counter, outs, bmw);
+    kern<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units, ctx->d_unit_counter,
+                                    outs, bmw);
     BBTC_CUDA(cudaGetLastError());
     plan->launches = 1;
   }

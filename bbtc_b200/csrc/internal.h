@@ -41,6 +41,7 @@ struct DevTile {
   const uint32_t* rp;
   const uint32_t* col;
   const uint2* rec;  // reversed tiles: pair range [word of v, end) in row u, per entry's forward edge (u, v)
+  const uint32_t* erow;  // row of entry 32 q, for q < ceil(nnz / 32)
   uint32_t H, W, nnz, maxdeg;
 };
 
@@ -81,7 +82,8 @@ struct BlockTiles {
   uint32_t* d_rp = nullptr;                    // row-pointer pool
   uint32_t* d_col = nullptr;                   // column pool
   void* d_rec = nullptr;                       // reversed tiles: forward-edge records (uint2), col-aligned
-  size_t rp_len = 0, col_len = 0;
+  uint32_t* d_erow = nullptr;                  // row index of every 32nd entry, per tile
+  size_t rp_len = 0, col_len = 0, erow_len = 0;
   cudaStream_t stream = nullptr;
   void release(cudaStream_t s);
 };
@@ -95,6 +97,7 @@ struct Plan {
   cudaStream_t stream = nullptr;   // stream the buffers were allocated on
   uint32_t total_units = 0;
   uint32_t launches = 0;
+  bool fused = false;              // every task is a fused task row
   cudaGraphExec_t exec = nullptr;
   bool captured = false;
   void release();

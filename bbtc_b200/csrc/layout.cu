@@ -193,6 +193,25 @@ __global__ void k_tile_offsets(const uint32_t* __restrict__ rp, const uint64_t* 
   }
 }
 
+// Row index of every 32nd entry: erow[t][x / 32] = the row holding entry x
+// of tile t, for x = 0, 32, 64, ... < nnz.  A work unit starting at a
+// multiple of 32 finds its first row with one load.  Every such x lies in
+// exactly one non-empty row, so each slot has one writer.  blockIdx.y = tile.
+__global__ void k_row_index(const uint32_t* __restrict__ rp, const uint64_t* __restrict__ rp_off,
+                            const uint32_t* __restrict__ cuts, uint32_t P, const uint64_t* __restrict__ col_off,
+                            uint32_t* __restrict__ erow) {
+  const uint32_t t = blockIdx.y;
+  if (col_off[t] == kNoSegment) return;
+  const uint32_t x = t / P;
+  const uint32_t H = cuts[x + 1] - cuts[x];
+  const uint32_t* __restrict__ r = rp + rp_off[t];
+  uint32_t* __restrict__ er = erow + col_off[t] / 32 + t;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < H; b += gridDim.x * blockDim.x) {
+    const uint32_t s = r[b], e = r[b + 1];
+    for (uint32_t q = (s + 31) & ~31u; q < e; q += 32) er[q >> 5] = b;
+  }
+}
+
 // Scatter tile-local column ids (and, for the reversed graph, the records of
 // the forward edges) into the column pool.
 __global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
@@ -336,11 +355,13 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   part_off[P] = cur;
   bt.rp_len = cur + 4;  // a 16-byte tail keeps rounded-up reads inside the pool
   bt.col_len = m + 4ull * T + 4;
+  bt.erow_len = bt.col_len / 32 + T + 1;  // tile t's index starts at col_off[t] / 32 + t
   {
     cudaError_t e1 = cudaMallocAsync(&bt.d_rp, bt.rp_len * sizeof(uint32_t), s);
     cudaError_t e2 = cudaMallocAsync(&bt.d_col, bt.col_len * sizeof(uint32_t), s);
     cudaError_t e3 = eids ? cudaMallocAsync(&bt.d_rec, bt.col_len * sizeof(uint2), s) : cudaSuccess;
-    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+    cudaError_t e4 = cudaMallocAsync(&bt.d_erow, bt.erow_len * sizeof(uint32_t), s);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess) {
       cudaGetLastError();
       bt.release(s);
       return fail(BBTC_ERR_NOMEM, "device allocation of the block-CSR pools failed");
@@ -378,6 +399,13 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   BBTC_CUDA(cudaGetLastError());
   k_tile_offsets<<<1, 32, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, st_nnz, d_coloff);
   BBTC_CUDA(cudaGetLastError());
+  {
+    uint32_t maxH = 1;
+    for (uint32_t x = 0; x < P; x++) maxH = std::max(maxH, cuts[x + 1] - cuts[x]);
+    const uint32_t gx = std::min<uint32_t>(64, (maxH + 255) / 256);
+    k_row_index<<<dim3(gx, T), 256, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, d_coloff, bt.d_erow);
+    BBTC_CUDA(cudaGetLastError());
+  }
   if (m > 0) {
     k_entry_scatter<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
                                          bt.d_col, eids, wpos, wptr, reinterpret_cast<uint2*>(bt.d_rec));
@@ -412,7 +440,8 @@ void BlockTiles::release(cudaStream_t s) {
   if (d_rp) cudaFreeAsync(d_rp, s);
   if (d_col) cudaFreeAsync(d_col, s);
   if (d_rec) cudaFreeAsync(d_rec, s);
-  d_rp = d_col = nullptr;
+  if (d_erow) cudaFreeAsync(d_erow, s);
+  d_rp = d_col = d_erow = nullptr;
   d_rec = nullptr;
 }
 
@@ -427,8 +456,9 @@ DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_
     d.rp = t.d_rp + t.rp_off[id];
     d.col = t.d_col + t.col_off[id];
     d.rec = t.d_rec ? reinterpret_cast<const uint2*>(t.d_rec) + t.col_off[id] : nullptr;
+    d.erow = t.d_erow + t.col_off[id] / 32 + id;
   } else {
-    d.rp = d.col = nullptr;
+    d.rp = d.col = d.erow = nullptr;
     d.rec = nullptr;
   }
   return d;
@@ -575,7 +605,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   g->layout_ms = ms;
   g->device_bytes = (g->fwd.rp_len + g->fwd.col_len + g->rev.rp_len + g->rev.col_len) * sizeof(uint32_t) +
                     g->rev.col_len * sizeof(uint2) + ((uint64_t)n + 1 + m) * sizeof(uint32_t) + 64 * sizeof(uint64_t) +
-                    m * sizeof(uint2) + ((uint64_t)n + 1) * sizeof(uint32_t);
+                    m * sizeof(uint2) + ((uint64_t)n + 1) * sizeof(uint32_t) +
+                    (g->fwd.erow_len + g->rev.erow_len) * sizeof(uint32_t);
   return BBTC_OK;
 }
 

@@ -46,7 +46,8 @@ uint64_t estimate_bytes(uint32_t n, uint64_t m, const std::vector<uint32_t>& cut
   const uint64_t P = cuts.size() - 1;
   uint64_t rp = 0;
   for (uint64_t x = 0; x < P; x++) rp += P * (((uint64_t)cuts[x + 1] - cuts[x] + 1 + 3) & ~3ull);
-  const uint64_t pools = 2 * 4 * (rp + 4) + 2 * 4 * (m + 4 * P * P + 4) + 8 * (m + 4 * P * P + 4);
+  const uint64_t pools = 2 * 4 * (rp + 4) + 2 * 4 * (m + 4 * P * P + 4) + 8 * (m + 4 * P * P + 4) +
+                        2 * 4 * (m / 32 + 2 * P * P + 2);
   const uint64_t csr = 4 * ((uint64_t)n + 1) + 4 * m;
   const uint64_t temps = 4 * (rp + 4) + 24 * m + 4 * ((uint64_t)n + 1) + (16ull << 20);
   return pools + csr + temps;

@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--kernel", default="auto")
     p.add_argument("--bitmap-words", type=int, default=0)
     p.add_argument("--unit-work", type=int, default=0)
+    p.add_argument("--occupancy", type=int, default=0)
+    p.add_argument("--warps", type=int, default=0)
+    p.add_argument("--autotune", action="store_true", help="sweep launch options first (cached)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -362,7 +365,13 @@ def main():
     layout_ms = st.info().layout_ms
     device_bytes = st.info().device_bytes
     o = options(mode="persistent", kernel=args.kernel, bitmap_words=args.bitmap_words, unit_work=args.unit_work,
-                cuda_graph=True)
+                cuda_graph=True, occupancy=args.occupancy, warps_per_block=args.warps)
+    tuned = None
+    if args.autotune:
+        from bbtc_b200 import autotune
+        o, tune_ms = autotune.tune(st)
+        o.use_cuda_graph = 1
+        tuned = {f: getattr(o, f) for f in ("bitmap_words", "warps_per_block", "unit_work", "occupancy")}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
     def timed_counts(opts, steps, warmup):
@@ -471,6 +480,8 @@ def main():
                    "kernel": args.kernel, "triangles": count if world == 1 else count_total,
                    "layout_ms": layout_ms, "device_bytes": device_bytes, "generate_s": round(gen_s, 2),
                    "l2": "block CSR larger than L2, plus a 256 MiB fill between timed steps (excluded)",
+                   "launch": {f: getattr(o, f) for f in ("bitmap_words", "warps_per_block", "unit_work",
+                                                         "occupancy")}, "autotuned": tuned is not None,
                    "parallelism": "replicas per GPU" if world > 1 else "single GPU"},
         "plain": plain,
         "e2e": e2e,

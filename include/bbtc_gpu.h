@@ -135,10 +135,11 @@ typedef struct bbtc_opts {
   int kernel;                /* bbtc_kernel */
   uint32_t bitmap_words;     /* shared bitmap / list words per warp: 0 = default (1024) */
   uint32_t warps_per_block;  /* 0 = default (8) */
-  uint32_t unit_work;        /* target probes per work unit, 0 = default */
+  uint32_t unit_work;        /* target probes per work unit, 0 = default (256 task rows, 8192 tasks) */
   uint32_t blocks_per_sm;    /* persistent grid = SMs x this, 0 = occupancy limit */
   int use_cuda_graph;        /* replay the launch sequence through a captured CUDA graph */
   int sort_tasks;            /* when tasks == NULL: 1 = cost-sorted descending (default) */
+  uint32_t occupancy;        /* persistent form: register budget for 4, 6 (default) or 8 blocks per SM */
 } bbtc_opts;
 
 void bbtc_opts_default(bbtc_opts* o);
@@ -178,6 +179,8 @@ typedef struct bbtc_tune_space {
   const uint32_t* unit_work;
   uint32_t n_unit_work;
   uint32_t repeats; /* timed counts per point, the median is kept (0 = 3) */
+  const uint32_t* occupancy;
+  uint32_t n_occupancy;
 } bbtc_tune_space;
 int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bbtc_opts* inout,
                   double* best_ms);
