@@ -350,7 +350,9 @@ class BBTc:
 # ---- request server (continuous batching) ----------------------------------
 class ServerOpts(c.Structure):
     _fields_ = [("hbm_budget", c.c_uint64), ("max_batch", c.c_uint32), ("max_requests", c.c_uint32),
-                ("loaders", c.c_uint32), ("reserved", c.c_uint32), ("count", Opts)]
+                ("loaders", c.c_uint32), ("reserved", c.c_uint32), ("count", Opts),
+                ("small_edges", c.c_uint64), ("large_blocks_per_sm", c.c_uint32), ("aging_ms", c.c_uint32),
+                ("pool_bytes", c.c_uint64)]
 
 
 class RequestInfo(c.Structure):
@@ -392,7 +394,8 @@ class Server:
     of a request are kept referenced here until the request is released."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch: int = 0, loaders: int = 0,
-                 opts: Opts | None = None):
+                 opts: Opts | None = None, small_edges: int = 0, large_blocks_per_sm: int = 0,
+                 aging_ms: int | None = None, pool_bytes: int = 0):
         L = _server_lib()
         so = ServerOpts()
         L.bbtc_server_opts_default(c.byref(so))
@@ -404,6 +407,14 @@ class Server:
             so.loaders = loaders
         if opts is not None:
             so.count = opts
+        if small_edges:
+            so.small_edges = small_edges
+        if large_blocks_per_sm:
+            so.large_blocks_per_sm = large_blocks_per_sm
+        if aging_ms is not None:
+            so.aging_ms = aging_ms
+        if pool_bytes:
+            so.pool_bytes = pool_bytes
         self._h = c.c_void_p()
         check(L.bbtc_server_create(device, c.byref(so), c.byref(self._h)))
         self._keep: dict[int, tuple] = {}

@@ -732,6 +732,7 @@ int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o) {
   if (sm > ctx->smem_optin)
     return fail(BBTC_ERR_ARG, "bitmap_words x warps_per_block needs " + std::to_string(sm) +
                                   " bytes of shared memory; the device allows " + std::to_string(ctx->smem_optin));
+  if (sm <= ctx->smem_set) return BBTC_OK;
   BBTC_CUDA(cudaFuncSetAttribute(k_count_queue<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_count_queue<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_count_queue<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -739,6 +740,7 @@ int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o) {
   BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_count_task, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  ctx->smem_set = sm;
   return BBTC_OK;
 }
 

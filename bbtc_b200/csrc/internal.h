@@ -111,6 +111,7 @@ struct bbtc_ctx {
   int sms = 0;
   size_t smem_optin = 0;
   uint32_t* d_unit_counter = nullptr;  // persistent-queue head (one word per launch slot)
+  size_t smem_set = 0;                 // dynamic shared memory the count kernels are opted in to
 };
 
 struct bbtc_graph {

@@ -3,14 +3,20 @@
 // No counterpart in the reference (it counts one graph per process).  A
 // request is a host CSR + cut vector; its answer is the exact count.
 //
-//   loader threads (each with its own stream): take the oldest pending
-//     request whose estimated device footprint fits the HBM budget, build its
-//     device block CSR (upload + layout), mark it ready.  A request that could
-//     never fit fails with BBTC_ERR_CAPACITY.
-//   launcher thread (its own stream): takes every ready graph (up to
+//   loader threads (each with its own high-priority stream): take a pending
+//     request whose estimated device footprint fits the HBM budget -- the
+//     smallest, or the oldest once it has waited aging_ms -- build its device
+//     block CSR (upload + layout), and queue it on its size class's lane.  A
+//     request that could never fit fails with BBTC_ERR_CAPACITY.  With two or
+//     more loaders the first one takes small requests only.
+//   two launcher threads (lanes), each with its own stream: lane 0 counts
+//     graphs of at most small_edges edges at the highest stream priority,
+//     lane 1 the larger ones with its persistent grid capped below the
+//     occupancy limit, so a small request never waits for a large count to
+//     drain the GPU.  A lane takes every ready graph of its class (up to
 //     max_batch), counts them in one persistent launch with one u64 slot per
 //     graph, publishes the counts, frees the graphs, returns their memory to
-//     the budget.
+//     the budget.  The device memory pool is grown once at creation.
 //
 // So requests that arrive while a launch is on the GPU are uploaded and laid
 // out on the loader streams at the same time, and join the next launch; the
@@ -74,44 +80,90 @@ void graph_release_on(bbtc_graph* g, cudaStream_t s);  // api.cu
 
 }  // namespace bbtc
 
+struct bbtc_server;
+
+namespace bbtc {
+namespace {
+
+// One launch lane: a launcher thread with its own stream, result slots and
+// ready queue.  Lane 0 counts the small graphs on a high-priority stream;
+// lane 1 the large ones, with its persistent grid capped so that lane 0's
+// launches (and the loaders' layout kernels) always find free block slots.
+struct Lane {
+  bbtc_ctx* ctx = nullptr;
+  std::deque<Request*> ready;
+  std::condition_variable cv;
+  std::thread th;
+  uint64_t* d_outs = nullptr;
+  std::vector<uint64_t> h_outs;
+  uint32_t blocks_per_sm = 0;  // 0: as many as fit
+  uint64_t launches = 0;
+};
+
+}  // namespace
+}  // namespace bbtc
+
 struct bbtc_server {
   bbtc_server_opts opts{};
   int device = 0;
   std::vector<bbtc_ctx*> load_ctx;
-  bbtc_ctx* run_ctx = nullptr;
   std::mutex mu;
-  std::condition_variable cv_load, cv_run, cv_done;
+  std::condition_variable cv_load, cv_done;
   std::deque<bbtc::Request*> pending;
-  std::deque<bbtc::Request*> ready;
+  bbtc::Lane lanes[2];
   std::unordered_map<uint64_t, bbtc::Request*> all;
   uint64_t next_id = 1;
   uint64_t in_use = 0;
   uint32_t loading = 0;
   bool stop = false;
   std::vector<std::thread> loaders;
-  std::thread launcher;
-  uint64_t* d_outs = nullptr;
-  std::vector<uint64_t> h_outs;
   // statistics
-  uint64_t launches = 0, counted = 0, max_batch_seen = 0;
+  uint64_t counted = 0, max_batch_seen = 0;
 };
 
 namespace bbtc {
 namespace {
 
-void loader_main(bbtc_server* s, bbtc_ctx* ctx) {
+constexpr size_t kPickScan = 4096;  // pending requests a loader looks at per pick
+
+uint32_t lane_of(const bbtc_server* s, const Request* r) { return r->m <= s->opts.small_edges ? 0u : 1u; }
+
+// The next request a loader takes, removed from `pending`, or nullptr.  Among
+// the requests the HBM budget admits (or that can never fit, and fail at
+// once): the oldest one that has waited `aging_ms` or more, else the one
+// with the fewest edges -- small requests overtake large loads, and large
+// ones are not starved.  A loader reserved for small requests sees only those.
+Request* pick(bbtc_server* s, bool small_only) {
+  const uint64_t now = now_ns();
+  const uint64_t aging = (uint64_t)s->opts.aging_ms * 1000000ull;
+  size_t best = SIZE_MAX, i = 0;
+  for (auto it = s->pending.begin(); it != s->pending.end() && i < kPickScan; ++it, ++i) {
+    const Request* r = *it;
+    if (small_only && lane_of(s, r) != 0) continue;
+    const bool never = r->reserved > s->opts.hbm_budget;
+    if (!never && s->in_use + r->reserved > s->opts.hbm_budget && s->in_use != 0) continue;
+    if (now - r->t_submit >= aging) {
+      best = i;
+      break;
+    }
+    if (best == SIZE_MAX || r->m < s->pending[best]->m) best = i;
+  }
+  if (best == SIZE_MAX) return nullptr;
+  Request* r = s->pending[best];
+  s->pending.erase(s->pending.begin() + (std::ptrdiff_t)best);
+  return r;
+}
+
+void loader_main(bbtc_server* s, bbtc_ctx* ctx, bool small_only) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
-    s->cv_load.wait(lk, [&] {
-      if (s->stop) return true;
-      if (s->pending.empty()) return false;
-      const Request* r = s->pending.front();
-      return s->in_use + r->reserved <= s->opts.hbm_budget || (s->in_use == 0);
-    });
-    if (s->stop) return;
-    Request* r = s->pending.front();
-    s->pending.pop_front();
+    Request* r = nullptr;
+    s->cv_load.wait(lk, [&] { return s->stop || (r = pick(s, small_only)) != nullptr; });
+    if (s->stop) {
+      if (r) s->pending.push_front(r);
+      return;
+    }
     if (r->reserved > s->opts.hbm_budget) {  // can never fit
       r->status = BBTC_ERR_CAPACITY;
       r->t_done = now_ns();
@@ -143,24 +195,26 @@ void loader_main(bbtc_server* s, bbtc_ctx* ctx) {
     r->g = g;
     r->status = 2;
     r->t_ready = now_ns();
-    s->ready.push_back(r);
-    s->cv_run.notify_one();
+    Lane& L = s->lanes[lane_of(s, r)];
+    L.ready.push_back(r);
+    L.cv.notify_one();
     s->cv_load.notify_all();
   }
 }
 
-void launcher_main(bbtc_server* s) {
+void launcher_main(bbtc_server* s, uint32_t lane) {
   cudaSetDevice(s->device);
-  bbtc_ctx* ctx = s->run_ctx;
+  Lane& L = s->lanes[lane];
+  bbtc_ctx* ctx = L.ctx;
   std::unique_lock<std::mutex> lk(s->mu);
   Plan plan;
   while (true) {
-    s->cv_run.wait(lk, [&] { return s->stop || !s->ready.empty(); });
-    if (s->stop && s->ready.empty()) break;
+    L.cv.wait(lk, [&] { return s->stop || !L.ready.empty(); });
+    if (s->stop && L.ready.empty()) break;
     std::vector<Request*> batch;
-    while (!s->ready.empty() && batch.size() < s->opts.max_batch) {
-      batch.push_back(s->ready.front());
-      s->ready.pop_front();
+    while (!L.ready.empty() && batch.size() < s->opts.max_batch) {
+      batch.push_back(L.ready.front());
+      L.ready.pop_front();
     }
     const uint64_t t_launch = now_ns();
     for (Request* r : batch) {
@@ -173,6 +227,7 @@ void launcher_main(bbtc_server* s) {
     for (Request* r : batch) gs.push_back(r->g);
     bbtc_opts o = s->opts.count;
     o.use_cuda_graph = 0;
+    if (L.blocks_per_sm && (!o.blocks_per_sm || o.blocks_per_sm > L.blocks_per_sm)) o.blocks_per_sm = L.blocks_per_sm;
     const bool fused = o.kernel == BBTC_KERNEL_FUSED || (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT);
     int rc = BBTC_OK;
     if (!fused) {
@@ -183,10 +238,10 @@ void launcher_main(bbtc_server* s) {
         bbtc_task_list(gs[i]->P, tl[i].data(), nt, &nt);
       }
     }
-    rc = count_enqueue(ctx, gs, tl, o, fused, s->d_outs, &plan, false);
+    rc = count_enqueue(ctx, gs, tl, o, fused, L.d_outs, &plan, false);
     if (rc == BBTC_OK) {
       const cudaError_t e =
-          cudaMemcpyAsync(s->h_outs.data(), s->d_outs, batch.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+          cudaMemcpyAsync(L.h_outs.data(), L.d_outs, batch.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                           ctx->stream);
       const cudaError_t e2 = e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
       if (e2 != cudaSuccess) rc = cuda_fail(e2, "server batch readback");
@@ -203,13 +258,13 @@ void launcher_main(bbtc_server* s) {
       r->batch = (uint32_t)batch.size();
       r->t_done = t;
       if (rc == BBTC_OK) {
-        r->count = s->h_outs[i];
+        r->count = L.h_outs[i];
         r->status = 4;
       } else {
         r->status = rc;
       }
     }
-    s->launches++;
+    L.launches++;
     s->counted += batch.size();
     s->max_batch_seen = std::max<uint64_t>(s->max_batch_seen, batch.size());
     s->cv_done.notify_all();
@@ -217,6 +272,15 @@ void launcher_main(bbtc_server* s) {
   }
   lk.unlock();
   plan.release();
+}
+
+// Give a context's stream the requested priority (lower numbers run first).
+int set_stream_priority(bbtc_ctx* c, int priority) {
+  cudaStream_t st = nullptr;
+  BBTC_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority));
+  cudaStreamDestroy(c->stream);
+  c->stream = st;
+  return BBTC_OK;
 }
 
 void fill_info(const Request* r, bbtc_request_info* info) {
@@ -245,6 +309,10 @@ void bbtc_server_opts_default(bbtc_server_opts* o) {
   o->max_requests = 1u << 20;
   o->loaders = 2;
   bbtc_opts_default(&o->count);
+  o->small_edges = 1ull << 22;
+  o->large_blocks_per_sm = 0;
+  o->aging_ms = 50;
+  o->pool_bytes = 0;
 }
 
 int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** out) {
@@ -258,27 +326,66 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
   if (!s->opts.max_requests) s->opts.max_requests = 1u << 20;
   if (!s->opts.loaders) s->opts.loaders = 2;
   s->opts.loaders = std::min<uint32_t>(s->opts.loaders, 16);
+  if (!s->opts.small_edges) s->opts.small_edges = 1ull << 22;
   s->device = device;
-  int rc = bbtc_ctx_create(device, &s->run_ctx);
+  int lo = 0, hi = 0;
+  int rc = BBTC_OK;
+  if (cudaSetDevice(device) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) {
+    cudaGetLastError();
+    lo = hi = 0;
+  }
+  // lane 0 (small graphs) and the loaders run at the highest stream priority
+  for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
+    rc = bbtc_ctx_create(device, &s->lanes[l].ctx);
+    if (rc == BBTC_OK) rc = set_stream_priority(s->lanes[l].ctx, l == 0 ? hi : lo);
+  }
   for (uint32_t i = 0; rc == BBTC_OK && i < s->opts.loaders; i++) {
     bbtc_ctx* c = nullptr;
     rc = bbtc_ctx_create(device, &c);
     if (rc == BBTC_OK) s->load_ctx.push_back(c);
+    if (rc == BBTC_OK) rc = set_stream_priority(c, hi);
   }
-  if (rc == BBTC_OK && cudaMalloc(&s->d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess) {
-    cudaGetLastError();
-    rc = fail(BBTC_ERR_NOMEM, "device allocation of the result slots failed");
+  for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
+    if (cudaMalloc(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(BBTC_ERR_NOMEM, "device allocation of the result slots failed");
+    }
   }
   if (rc != BBTC_OK) {
     for (auto* c : s->load_ctx) bbtc_ctx_destroy(c);
-    if (s->run_ctx) bbtc_ctx_destroy(s->run_ctx);
-    if (s->d_outs) cudaFree(s->d_outs);
+    for (auto& L : s->lanes) {
+      if (L.ctx) bbtc_ctx_destroy(L.ctx);
+      if (L.d_outs) cudaFree(L.d_outs);
+    }
     delete s;
     return rc;
   }
-  s->h_outs.assign(s->opts.max_batch, 0);
-  for (auto* c : s->load_ctx) s->loaders.emplace_back(loader_main, s, c);
-  s->launcher = std::thread(launcher_main, s);
+  {
+    // the large lane leaves a third of the occupancy target (at least one
+    // block per SM) to the small lane
+    const uint32_t occ = s->opts.count.occupancy >= 8 ? 8 : (s->opts.count.occupancy >= 6 ? 6 : 4);
+    s->lanes[1].blocks_per_sm =
+        s->opts.large_blocks_per_sm ? s->opts.large_blocks_per_sm : occ - std::max<uint32_t>(1, occ / 3);
+  }
+  {
+    // grow the device's memory pool once, now: a pool that grows while loads
+    // and counts run stalled every loader for hundreds of milliseconds
+    const uint64_t want =
+        s->opts.pool_bytes ? s->opts.pool_bytes : std::min<uint64_t>(s->opts.hbm_budget, 48ull << 30);
+    cudaStream_t st = s->lanes[0].ctx->stream;
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, want, st) == cudaSuccess) {
+      cudaFreeAsync(p, st);
+      cudaStreamSynchronize(st);
+    } else {
+      cudaGetLastError();  // not fatal: the pool grows on demand instead
+    }
+  }
+  for (auto& L : s->lanes) L.h_outs.assign(s->opts.max_batch, 0);
+  // with two or more loaders, the first takes small requests only
+  for (size_t i = 0; i < s->load_ctx.size(); i++)
+    s->loaders.emplace_back(loader_main, s, s->load_ctx[i], i == 0 && s->load_ctx.size() > 1);
+  for (uint32_t l = 0; l < 2; l++) s->lanes[l].th = std::thread(launcher_main, s, l);
   *out = s;
   return BBTC_OK;
 }
@@ -296,18 +403,21 @@ int bbtc_server_destroy(bbtc_server* s) {
     s->cv_done.wait(lk, [&] { return s->loading == 0; });
     s->stop = true;
     s->cv_load.notify_all();
-    s->cv_run.notify_all();
+    for (auto& L : s->lanes) L.cv.notify_all();
   }
   for (auto& t : s->loaders) t.join();
-  s->launcher.join();
+  for (auto& L : s->lanes) L.th.join();
   for (auto& kv : s->all) {
-    if (kv.second->g) graph_release_on(kv.second->g, s->run_ctx->stream);
+    if (kv.second->g) graph_release_on(kv.second->g, s->lanes[0].ctx->stream);
     delete kv.second;
   }
   cudaSetDevice(s->device);
-  cudaFree(s->d_outs);
+  for (auto& L : s->lanes) {
+    cudaStreamSynchronize(L.ctx->stream);
+    cudaFree(L.d_outs);
+  }
   for (auto* c : s->load_ctx) bbtc_ctx_destroy(c);
-  bbtc_ctx_destroy(s->run_ctx);
+  for (auto& L : s->lanes) bbtc_ctx_destroy(L.ctx);
   delete s;
   return BBTC_OK;
 }
@@ -338,7 +448,7 @@ int bbtc_submit(bbtc_server* s, uint32_t n, const uint32_t* indptr, const uint32
   s->all[r->id] = r;
   s->pending.push_back(r);
   *req_id = r->id;
-  s->cv_load.notify_one();
+  s->cv_load.notify_all();  // a loader reserved for small requests may not take this one
   return BBTC_OK;
 }
 
@@ -383,11 +493,11 @@ int bbtc_release(bbtc_server* s, uint64_t req_id) {
 int bbtc_server_stats_get(bbtc_server* s, bbtc_server_stats* st) {
   if (!s || !st) return fail(BBTC_ERR_ARG, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);
-  st->launches = s->launches;
+  st->launches = s->lanes[0].launches + s->lanes[1].launches;
   st->counted = s->counted;
   st->max_batch = s->max_batch_seen;
   st->pending = s->pending.size();
-  st->ready = s->ready.size();
+  st->ready = s->lanes[0].ready.size() + s->lanes[1].ready.size();
   st->device_bytes_in_use = s->in_use;
   return BBTC_OK;
 }

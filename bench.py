@@ -71,6 +71,9 @@ def parse():
     p.add_argument("--rate", type=float, default=1000.0, help="serve: requests per second")
     p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     p.add_argument("--serve-max-scale", type=int, default=22)
+    p.add_argument("--loaders", type=int, default=4, help="serve: loader threads")
+    p.add_argument("--pin", type=int, default=1, help="serve: request buffers in page-locked host memory")
+    p.add_argument("--trace", default="", help="serve: write every request's stage timestamps to this JSON file")
     return p.parse_args()
 
 
@@ -271,7 +274,18 @@ def run_serve(args):
     arrivals = np.cumsum(gaps)
     scales = np.minimum(12 + rng.geometric(0.3, size=n_req) - 1, args.serve_max_scale)
     picks = [pool[int(s)][int(rng.integers(len(pool[int(s)])))] for s in scales]
-    srv = Server(0, loaders=4)
+    pinned = []
+    if args.pin:
+        # request buffers in page-locked memory, as a serving front end that
+        # receives requests into pinned buffers holds them
+        import torch
+        rt = torch.cuda.cudart()
+        for gs in pool.values():
+            for g, _ in gs:
+                for a in (g.indptr, g.indices):
+                    if a.nbytes and rt.cudaHostRegister(a.ctypes.data, a.nbytes, 0) == 0:
+                        pinned.append(a)
+    srv = Server(0, loaders=args.loaders)
     # warm-up: one request per scale
     for s in sorted(pool):
         g, c = pool[s][0]
@@ -291,6 +305,8 @@ def run_serve(args):
     th.start()
     lat, lat18, edges, first_sub, last_done = [], [], 0, None, 0
     stages = {"queue": [], "load": [], "ready_wait": [], "count": []}
+    by_scale = {}
+    trace = []
     for i in range(n_req):
         while ids[i] is None:
             time.sleep(0.0002)
@@ -304,6 +320,10 @@ def run_serve(args):
         stages["count"].append((info.done_ns - info.launch_ns) / 1e6)
         if scales[i] <= 18:
             lat18.append(ms)
+        by_scale.setdefault(int(scales[i]), []).append(
+            (ms, (info.ready_ns - info.load_ns) / 1e6, (info.done_ns - info.launch_ns) / 1e6))
+        trace.append((int(scales[i]), int(picks[i][0].m), info.submit_ns, info.load_ns, info.ready_ns, info.launch_ns,
+                      info.done_ns, info.batch))
         edges += picks[i][0].m
         first_sub = info.submit_ns if first_sub is None else min(first_sub, info.submit_ns)
         last_done = max(last_done, info.done_ns)
@@ -311,19 +331,33 @@ def run_serve(args):
     th.join()
     stats = srv.stats()
     srv.close()
+    if args.trace:
+        with open(args.trace, "w") as f:
+            json.dump({"fields": ["scale", "m", "submit_ns", "load_ns", "ready_ns", "launch_ns", "done_ns", "batch"],
+                       "requests": trace}, f)
+    if pinned:
+        import torch
+        rt = torch.cuda.cudart()
+        for a in pinned:
+            rt.cudaHostUnregister(a.ctypes.data)
     span = (last_done - first_sub) / 1e9
     res = {"metric": METRIC, "value": edges / span, "unit": UNIT, "n_gpus": 1, "steps": n_req, "warmup": len(pool),
            "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "u32", "data": "synthetic",
            "config": {"workload": f"serving: Poisson {args.rate:g} req/s for {args.duration:g} s, R-MAT scale "
                                   f"12+Geom(0.3) <= {args.serve_max_scale}, ef 16", "requests": n_req,
-                      "generate_s": round(gen_s, 1), "launches": stats.launches, "max_batch": stats.max_batch},
+                      "generate_s": round(gen_s, 1), "launches": stats.launches, "max_batch": stats.max_batch,
+                      "loaders": args.loaders, "pinned_requests": bool(pinned)},
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "p50_scale_le_18": float(np.percentile(lat18, 50)) if lat18 else None,
                           "p99_scale_le_18": float(np.percentile(lat18, 99)) if lat18 else None,
                           "definition": "bbtc_submit -> count in host memory (server steady clock)"},
            "stages_ms_p50_p99": {k: [float(np.percentile(v, 50)), float(np.percentile(v, 99))]
-                                 for k, v in stages.items()}}
+                                 for k, v in stages.items()},
+           "by_scale_p50_ms": {s: {"n": len(v), "latency": float(np.percentile([x[0] for x in v], 50)),
+                                   "load": float(np.percentile([x[1] for x in v], 50)),
+                                   "count": float(np.percentile([x[2] for x in v], 50))}
+                               for s, v in sorted(by_scale.items())}}
     print(json.dumps(res), flush=True)
 
 

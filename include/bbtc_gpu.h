@@ -231,6 +231,11 @@ typedef struct bbtc_server_opts {
   uint32_t loaders;       /* loader threads, each with its own stream (0 = 2) */
   uint32_t reserved;
   bbtc_opts count;        /* launch options of every batch */
+  uint64_t small_edges;   /* graphs of at most this many edges use the high-priority lane (0 = 2^22) */
+  uint32_t large_blocks_per_sm; /* persistent blocks per SM of the large lane (0 = occupancy minus a third) */
+  uint32_t aging_ms;      /* a request waiting this long is loaded before smaller ones (default 50) */
+  uint64_t pool_bytes;    /* the device memory pool is grown to this size at creation, so loads never
+                             wait for it to grow (0 = min(hbm_budget, 48 GiB)) */
 } bbtc_server_opts;
 typedef struct bbtc_request_info {
   uint64_t count;     /* exact count once status == 1 */

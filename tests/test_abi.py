@@ -63,3 +63,31 @@ def test_host_library_exports():
     lib = _lib.host()
     for n in ("bbtcg_rmat", "bbtcg_chung_lu", "bbtcg_rgg", "bbtcg_from_pairs", "bbtcp_cuts"):
         assert hasattr(lib, n)
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes mirror has the size and field offsets gcc gives the C struct."""
+    import shutil
+    import subprocess
+    from bbtc_b200 import autotune
+    mirrors = {"bbtc_task": core.Task, "bbtc_opts": core.Opts, "bbtc_graph_info": core.GraphInfo,
+               "bbtc_tune_space": autotune.TuneSpace, "bbtc_csr_dev": core.CsrDev,
+               "bbtc_server_opts": core.ServerOpts, "bbtc_request_info": core.RequestInfo,
+               "bbtc_server_stats": core.ServerStats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "bbtc_gpu.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'  printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    cc = shutil.which("gcc") or shutil.which("cc")
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
