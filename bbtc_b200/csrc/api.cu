@@ -164,6 +164,13 @@ int bbtc_ctx_create(int device, bbtc_ctx** out) {
     delete c;
     return cuda_fail(e, "cudaMalloc");
   }
+  e = cudaMallocHost(&c->h_stage, kStageBytes);
+  if (e != cudaSuccess) {
+    cudaFree(c->d_unit_counter);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return cuda_fail(e, "cudaMallocHost");
+  }
   *out = c;
   return BBTC_OK;
 }
@@ -173,6 +180,7 @@ int bbtc_ctx_destroy(bbtc_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->d_unit_counter) cudaFree(ctx->d_unit_counter);
+  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return BBTC_OK;
@@ -244,6 +252,7 @@ int bbtc_graph_info_get(const bbtc_graph* g, bbtc_graph_info* info) {
 int bbtc_graph_tile_stats(const bbtc_graph* g, uint32_t* nnz, uint32_t* height, uint32_t* width, float* tile_deg,
                           uint32_t* max_deg) {
   if (!g) return fail(BBTC_ERR_ARG, "NULL graph");
+  BBTC_TRY(ensure_fwd(const_cast<bbtc_graph*>(g)));
   const uint32_t P = g->P;
   for (uint32_t x = 0; x < P; x++)
     for (uint32_t y = 0; y < P; y++) {
@@ -276,7 +285,7 @@ int bbtc_sort_tasks(const bbtc_graph* g, bbtc_task* tasks, uint32_t ntasks, int 
   if (!g || (ntasks && !tasks)) return fail(BBTC_ERR_ARG, "NULL argument");
   const uint32_t P = g->P;
   std::vector<float> deg(P * P);
-  bbtc_graph_tile_stats(g, nullptr, nullptr, nullptr, deg.data(), nullptr);
+  BBTC_TRY(bbtc_graph_tile_stats(g, nullptr, nullptr, nullptr, deg.data(), nullptr));
   for (uint32_t q = 0; q < ntasks; q++)
     if (tasks[q].ab >= P * P || tasks[q].bc >= P * P || tasks[q].ac >= P * P)
       return fail(BBTC_ERR_ARG, "task names a tile outside the P x P grid");
@@ -325,8 +334,10 @@ static int count_async_impl(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks
   const bool fused = !tasks && (o.kernel == BBTC_KERNEL_FUSED ||
                                 (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT));
   BBTC_CUDA(cudaSetDevice(ctx->device));
+  if (!fused) BBTC_TRY(ensure_fwd(g));  // task-list counting reads the forward block CSR
   std::vector<std::vector<bbtc_task>> tl(1);
-  if (tasks) tl[0].assign(tasks, tasks + ntasks); else tl[0] = default_tasks(g, o.sort_tasks != 0);
+  // fused task rows run every task whatever the order: no sort (it would need the forward tiles)
+  if (tasks) tl[0].assign(tasks, tasks + ntasks); else tl[0] = default_tasks(g, !fused && o.sort_tasks != 0);
   // border b >= 0: tasks [0, b) are queued ahead of the rest; with one device queue in list
   // order that is the list order itself, so the value only has to be in range.
   std::vector<bbtc_graph*> gs{g};
@@ -358,8 +369,10 @@ int bbtc_count_async(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint3
 int bbtc_count_wait(bbtc_ctx* ctx, bbtc_graph* g, uint64_t* out) {
   if (!ctx || !g || !out) return fail(BBTC_ERR_ARG, "NULL argument");
   BBTC_CUDA(cudaSetDevice(ctx->device));
-  BBTC_CUDA(cudaMemcpyAsync(out, g->d_count, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  uint64_t* h = reinterpret_cast<uint64_t*>(ctx->h_stage + kStageOut);
+  BBTC_CUDA(cudaMemcpyAsync(h, g->d_count, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
   BBTC_CUDA(cudaStreamSynchronize(ctx->stream));
+  *out = *h;
   return BBTC_OK;
 }
 
@@ -454,9 +467,11 @@ int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, cons
   BBTC_CUDA(cudaSetDevice(ctx->device));
   std::vector<bbtc_graph*> gs(graphs, graphs + ng);
   std::vector<std::vector<bbtc_task>> tl(ng);
+  const bool fused_all = o.kernel == BBTC_KERNEL_FUSED || (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT);
   for (uint32_t i = 0; i < ng; i++) {
     if (!gs[i] || gs[i]->ctx != ctx) return fail(BBTC_ERR_ARG, "graph is NULL or belongs to another context");
-    tl[i] = default_tasks(gs[i], o.sort_tasks != 0);
+    if (!fused_all) BBTC_TRY(ensure_fwd(gs[i]));
+    tl[i] = default_tasks(gs[i], !fused_all && o.sort_tasks != 0);
   }
   uint64_t* d_outs = nullptr;
   BBTC_CUDA(cudaMallocAsync(&d_outs, ng * sizeof(uint64_t), ctx->stream));
@@ -471,9 +486,12 @@ int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, cons
   const bool fused = o.kernel == BBTC_KERNEL_FUSED || (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT);
   int rc = count_enqueue(ctx, gs, tl, o, fused, d_outs, &plan, false);
   if (rc == BBTC_OK) {
-    cudaError_t e = cudaMemcpyAsync(outs, d_outs, ng * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream);
+    const bool staged = (size_t)ng * sizeof(uint64_t) <= kStageBytes - kStageOut;
+    uint64_t* h = staged ? reinterpret_cast<uint64_t*>(ctx->h_stage + kStageOut) : outs;
+    cudaError_t e = cudaMemcpyAsync(h, d_outs, ng * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) rc = cuda_fail(e, "batch readback");
+    else if (staged) std::memcpy(outs, h, ng * sizeof(uint64_t));
   }
   for (uint32_t i = 0; i < ng; i++) gs[i]->last_launches = plan.launches;
   plan.release();

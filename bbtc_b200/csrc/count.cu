@@ -405,6 +405,12 @@ __device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_
   return acc;
 }
 
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t id;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(id));
+  return id;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(FULL, v, d);
@@ -424,8 +430,10 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_count_queue(const DevTask* __restrict__ tasks,
                                                         const uint32_t* __restrict__ prefix, uint32_t ntasks,
                                                         uint32_t total_units, uint32_t* __restrict__ head,
-                                                        unsigned long long* __restrict__ outs, uint32_t bm_words) {
+                                                        unsigned long long* __restrict__ outs, uint32_t bm_words,
+                                                        uint32_t spare_sms) {
   extern __shared__ __align__(16) uint32_t sh[];
+  if (spare_sms && blockIdx.x != 0 && sm_id() < spare_sms) return;  // block 0 stays: the queue always drains
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
   uint32_t* sstart = bm + bm_words;
@@ -613,8 +621,10 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __restrict__ tasks,
                                                         const uint32_t* __restrict__ prefix, uint32_t ntasks,
                                                         uint32_t total_units, uint32_t* __restrict__ head,
-                                                        unsigned long long* __restrict__ outs, uint32_t bm_words) {
+                                                        unsigned long long* __restrict__ outs, uint32_t bm_words,
+                                                        uint32_t spare_sms) {
   extern __shared__ __align__(16) uint32_t sh[];
+  if (spare_sms && blockIdx.x != 0 && sm_id() < spare_sms) return;  // block 0 stays: the queue always drains
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
   uint32_t* sstart = bm + bm_words;
@@ -749,9 +759,10 @@ static double part_row_len(const bbtc_graph* g, uint32_t i) {
   uint64_t z = 0;
   uint32_t rows = 1;
   for (uint32_t k = 0; k < g->P; k++) {
-    z += g->fwd.nnz[i * g->P + k];
-    rows = std::max(rows, g->fwd.nerows[i * g->P + k]);
+    z += g->rev.nnz[k * g->P + i];  // reversed tile (k, i) holds the edges of forward tile (i, k)
+    if (g->fwd_built) rows = std::max(rows, g->fwd.nerows[i * g->P + k]);
   }
+  if (!g->fwd_built) rows = std::max<uint32_t>(1, g->cuts[i + 1] - g->cuts[i]);
   return (double)z / rows;
 }
 
@@ -762,8 +773,8 @@ static double part_row_len(const bbtc_graph* g, uint32_t i) {
 static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<std::vector<bbtc_task>>& tasks,
                      const bbtc_opts& o, bool fused, Plan* plan) {
   const uint32_t bmw = norm_bm_words(o.bitmap_words);
-  // default unit size: task rows of the fused form run best as 32-entry
-  // units (the floor below); explicit task lists as units of ~8192 probes
+  // default unit size: task rows of the fused form run as 32-entry units
+  // (below); explicit task lists as units of ~8192 probes
   const uint32_t unit_work = o.unit_work ? o.unit_work : (fused ? 256 : 8192);
   std::vector<DevTask> list;
   std::vector<double> cost;
@@ -780,7 +791,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
     if (fused) {
       for (uint32_t i = 0; i < P; i++)
         for (uint32_t j = i; j < P; j++) {
-          if (!g->fwd.nnz[i * P + j]) continue;
+          if (!g->rev.nnz[j * P + i]) continue;  // forward tile (i, j) is empty
           DevTask d{};
           d.rows = dev_tile(g->rev, g->cuts, j, i);
           d.kind = kFusedRow;
@@ -790,6 +801,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
           d.g_words = reinterpret_cast<const uint2*>(g->d_words);
           d.pivot_base = g->cuts[j];
           add(d, 0.5 * part_row_len(g, i));
+          if (!o.unit_work) list.back().unit_edges = 32;  // the measured best: one probe batch per unit
         }
       continue;
     }
@@ -851,6 +863,14 @@ void Plan::release() {
   d_tasks = nullptr;
   d_prefix = nullptr;
   cap = 0;
+  if (h_done) {
+    cudaEventSynchronize(h_done);  // no upload still reads h_buf
+    cudaEventDestroy(h_done);
+    h_done = nullptr;
+  }
+  if (h_buf) cudaFreeHost(h_buf);
+  h_buf = nullptr;
+  h_cap = 0;
 }
 
 static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint64_t* d_outs, uint32_t nouts) {
@@ -880,10 +900,13 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
     BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, sm));
     per_sm = std::max(1, per_sm);
     if (o.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)o.blocks_per_sm);
-    const uint32_t grid = ctx->sms * per_sm;
+    // no more blocks than the queue has units for a warp each (a small batch
+    // leaves the rest of the GPU to other streams)
+    const uint64_t want = ((uint64_t)plan->total_units + wpb - 1) / wpb;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ctx->sms * per_sm, want));
     BBTC_CUDA(cudaMemsetAsync(ctx->d_unit_counter, 0, sizeof(uint32_t), s));
     kern<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units, ctx->d_unit_counter,
-                                    outs, bmw);
+                                    outs, bmw, o.spare_sms);
     BBTC_CUDA(cudaGetLastError());
     plan->launches = 1;
   }
@@ -913,11 +936,24 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
         }
         plan->cap = cap;
       }
-      BBTC_CUDA(cudaMemcpyAsync(plan->d_tasks, plan->tasks.data(), nt * sizeof(DevTask), cudaMemcpyHostToDevice, s));
-      // pageable sources: the copies are staged before cudaMemcpyAsync returns,
-      // and plan->tasks / prefix live until the plan is rebuilt
-      BBTC_CUDA(cudaMemcpyAsync(plan->d_prefix, plan->prefix.data(), (nt + 1) * sizeof(uint32_t),
-                                cudaMemcpyHostToDevice, s));
+      // upload from pinned staging (a pageable copy would go through the
+      // driver's shared staging buffers, which other threads' copies hold)
+      const size_t tb = nt * sizeof(DevTask), pb = (nt + 1) * sizeof(uint32_t);
+      if (plan->h_done) BBTC_CUDA(cudaEventSynchronize(plan->h_done));  // the last upload has read h_buf
+      if (tb + pb > plan->h_cap) {
+        if (plan->h_buf) cudaFreeHost(plan->h_buf);
+        plan->h_buf = nullptr;
+        plan->h_cap = 0;
+        const size_t want = std::max<size_t>(tb + pb, 64 << 10) * 2;
+        BBTC_CUDA(cudaMallocHost(&plan->h_buf, want));
+        plan->h_cap = want;
+      }
+      if (!plan->h_done) BBTC_CUDA(cudaEventCreateWithFlags(&plan->h_done, cudaEventDisableTiming));
+      std::memcpy(plan->h_buf, plan->tasks.data(), tb);
+      std::memcpy(plan->h_buf + tb, plan->prefix.data(), pb);
+      BBTC_CUDA(cudaMemcpyAsync(plan->d_tasks, plan->h_buf, tb, cudaMemcpyHostToDevice, s));
+      BBTC_CUDA(cudaMemcpyAsync(plan->d_prefix, plan->h_buf + tb, pb, cudaMemcpyHostToDevice, s));
+      BBTC_CUDA(cudaEventRecord(plan->h_done, s));
     }
     plan->captured = false;
   }

@@ -98,6 +98,9 @@ struct Plan {
   uint32_t total_units = 0;
   uint32_t launches = 0;
   bool fused = false;              // every task is a fused task row
+  char* h_buf = nullptr;           // pinned staging of the task queue's upload
+  size_t h_cap = 0;
+  cudaEvent_t h_done = nullptr;    // recorded after the last upload from h_buf
   cudaGraphExec_t exec = nullptr;
   bool captured = false;
   void release();
@@ -112,7 +115,22 @@ struct bbtc_ctx {
   size_t smem_optin = 0;
   uint32_t* d_unit_counter = nullptr;  // persistent-queue head (one word per launch slot)
   size_t smem_set = 0;                 // dynamic shared memory the count kernels are opted in to
+  uint32_t layout_blocks_per_sm = 8;   // grid cap of the layout kernels (256 threads a block)
+  // Page-locked staging for the small control copies (cut vectors, tile
+  // offsets and statistics, counts).  A copy to or from pageable memory is
+  // staged by the driver through buffers every thread shares, so one that
+  // waited for a long kernel on its stream held up the copies of all other
+  // threads; copies from pinned memory wait only for their own stream.
+  char* h_stage = nullptr;
 };
+
+// Regions of bbtc_ctx::h_stage (one graph build or count at a time per context).
+constexpr size_t kStageBytes = 1u << 20;
+constexpr size_t kStageCuts = 0;          // cut vector, <= (64 + 1) x 4 bytes
+constexpr size_t kStageBad = 3072;        // validation flags
+constexpr size_t kStageOff[2] = {4096, 40960};  // per block CSR: tile + part row offsets (<= 33,288 bytes)
+constexpr size_t kStageStats = 81920;     // tile statistics of both block CSRs (<= 163,840 bytes)
+constexpr size_t kStageOut = 262144;      // counts read back (<= 98,304 of them)
 
 struct bbtc_graph {
   bbtc_ctx* ctx = nullptr;
@@ -127,6 +145,7 @@ struct bbtc_graph {
   uint64_t* d_count = nullptr;  // result slot
   uint64_t device_bytes = 0;
   double layout_ms = 0;
+  bool fwd_built = false;         // the forward block CSR is built on first use (task-list counting, tile stats)
   uint32_t last_launches = 0;
   std::map<std::string, std::unique_ptr<bbtc::Plan>> plans;  // cached queues keyed by request
 };
@@ -137,6 +156,8 @@ namespace bbtc {
 // indptr / indices are host memory when `host`, else device memory of the
 // context's device; the graph keeps its own device copy either way.
 int build_layout(bbtc_graph* g, const uint32_t* indptr, const uint32_t* indices, bool host);
+// Build g's forward block CSR if it is not built yet (on g's context stream; synchronises it).
+int ensure_fwd(bbtc_graph* g);
 DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_t x, uint32_t y);
 
 // count.cu

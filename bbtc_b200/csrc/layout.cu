@@ -374,8 +374,13 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   BBTC_TRY(dalloc(base, T * sizeof(uint32_t), s));
   uint64_t* d_rp_off = offs.as<uint64_t>();
   uint64_t* d_part_off = d_rp_off + T;
-  BBTC_CUDA(cudaMemcpyAsync(d_rp_off, bt.rp_off.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-  BBTC_CUDA(cudaMemcpyAsync(d_part_off, part_off.data(), (P + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  {
+    // through this block CSR's own pinned region: it is not written again before the build's final sync
+    uint64_t* h = reinterpret_cast<uint64_t*>(ctx->h_stage + kStageOff[eids ? 1 : 0]);
+    std::memcpy(h, bt.rp_off.data(), T * sizeof(uint64_t));
+    std::memcpy(h + T, part_off.data(), (P + 1) * sizeof(uint64_t));
+    BBTC_CUDA(cudaMemcpyAsync(d_rp_off, h, (T + P + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  }
   BBTC_CUDA(cudaMemsetAsync(counts.p, 0, bt.rp_len * sizeof(uint32_t), s));
   BBTC_CUDA(cudaMemsetAsync(bt.d_col, 0, bt.col_len * sizeof(uint32_t), s));
   BBTC_CUDA(cudaMemsetAsync(d_stats, 0, 4 * T * sizeof(uint32_t), s));
@@ -414,24 +419,43 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   return BBTC_OK;
 }
 
-int fetch_stats(BlockTiles& a, BlockTiles& b, const uint32_t* d_stats_a, const uint64_t* d_coloff_a,
+// Read back the tile statistics of one or two block CSRs (a may be null) with one sync.
+int fetch_stats(bbtc_ctx* ctx, BlockTiles* a, BlockTiles& b, const uint32_t* d_stats_a, const uint64_t* d_coloff_a,
                 const uint32_t* d_stats_b, const uint64_t* d_coloff_b, cudaStream_t s) {
-  const uint32_t T = a.P * a.P;
-  std::vector<uint32_t> ha(3 * T), hb(3 * T);
-  BBTC_CUDA(cudaMemcpyAsync(ha.data(), d_stats_a, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  BBTC_CUDA(cudaMemcpyAsync(hb.data(), d_stats_b, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  a.col_off.assign(T, kNoSegment);
-  b.col_off.assign(T, kNoSegment);
-  BBTC_CUDA(cudaMemcpyAsync(a.col_off.data(), d_coloff_a, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-  BBTC_CUDA(cudaMemcpyAsync(b.col_off.data(), d_coloff_b, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  const uint32_t T = b.P * b.P;
+  // pinned staging: [coloff a | coloff b | stats a | stats b]
+  uint64_t* hc = reinterpret_cast<uint64_t*>(ctx->h_stage + kStageStats);
+  uint32_t* hs = reinterpret_cast<uint32_t*>(hc + 2 * T);
+  if (a) {
+    BBTC_CUDA(cudaMemcpyAsync(hc, d_coloff_a, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    BBTC_CUDA(cudaMemcpyAsync(hs, d_stats_a, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  }
+  BBTC_CUDA(cudaMemcpyAsync(hc + T, d_coloff_b, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  BBTC_CUDA(cudaMemcpyAsync(hs + 3 * T, d_stats_b, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   BBTC_CUDA(cudaStreamSynchronize(s));
-  for (auto* p : {&a, &b}) {
-    const auto& h = p == &a ? ha : hb;
-    p->nnz.assign(h.begin(), h.begin() + T);
-    p->maxdeg.assign(h.begin() + T, h.begin() + 2 * T);
-    p->nerows.assign(h.begin() + 2 * T, h.end());
+  for (BlockTiles* p : {a, &b}) {
+    if (!p) continue;
+    const uint64_t* c = p == a ? hc : hc + T;
+    const uint32_t* h = p == a ? hs : hs + 3 * T;
+    p->col_off.assign(c, c + T);
+    p->nnz.assign(h, h + T);
+    p->maxdeg.assign(h + T, h + 2 * T);
+    p->nerows.assign(h + 2 * T, h + 3 * T);
   }
   return BBTC_OK;
+}
+
+// Layout kernels are grid-stride loops: no more blocks than the largest array
+// needs (a tiny graph's layout leaves the GPU to others), at most the
+// context's cap.
+int layout_grid(const bbtc_ctx* ctx, uint32_t n, uint64_t m, uint32_t P) {
+  const uint64_t span = std::max<uint64_t>(m, (uint64_t)P * ((uint64_t)n + P));
+  return (int)std::min<uint64_t>((uint64_t)ctx->sms * ctx->layout_blocks_per_sm,
+                                 std::max<uint64_t>(ctx->sms, (span + 2047) / 2048));
+}
+
+uint64_t block_bytes(const BlockTiles& t, bool rec) {
+  return (t.rp_len + t.col_len + t.erow_len) * sizeof(uint32_t) + (rec ? t.col_len * sizeof(uint2) : 0);
 }
 
 }  // namespace
@@ -471,7 +495,7 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   const uint64_t m = g->m;
   const uint32_t P = g->P;
   const uint32_t T = P * P;
-  const int grid = ctx->sms * 8;
+  const int grid = layout_grid(ctx, n, m, P);
   cudaEvent_t ev0, ev1;
   BBTC_CUDA(cudaEventCreate(&ev0));
   BBTC_CUDA(cudaEventCreate(&ev1));
@@ -499,15 +523,17 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   const uint32_t* d_indptr = g->d_indptr;
   const uint32_t* d_indices = g->d_indices;
 
-  DevBuf d_cuts, bad, rows, stats, coloff, stats_r, coloff_r;
+  DevBuf d_cuts, bad, rows, stats_r, coloff_r;
   BBTC_TRY(dalloc(d_cuts, g->cuts.size() * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(bad, sizeof(uint32_t), s));
   BBTC_TRY(dalloc(rows, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
-  BBTC_TRY(dalloc(stats, 4 * T * sizeof(uint32_t), s));
-  BBTC_TRY(dalloc(coloff, T * sizeof(uint64_t), s));
   BBTC_TRY(dalloc(stats_r, 4 * T * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(coloff_r, T * sizeof(uint64_t), s));
-  BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, g->cuts.data(), g->cuts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  {
+    uint32_t* h = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageCuts);
+    std::memcpy(h, g->cuts.data(), g->cuts.size() * sizeof(uint32_t));
+    BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, h, g->cuts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  }
   BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
   uint32_t hbad = 0;
   if (n > 0) {
@@ -516,8 +542,10 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     BBTC_CUDA(cudaGetLastError());
     k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>());
     BBTC_CUDA(cudaGetLastError());
-    BBTC_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    uint32_t* hb = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageBad);
+    BBTC_CUDA(cudaMemcpyAsync(hb, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     BBTC_CUDA(cudaStreamSynchronize(s));
+    hbad = *hb;
   }
   if (hbad) {
     std::string why;
@@ -529,8 +557,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     return fail(BBTC_ERR_INPUT, "CSR breaks the input contract:" + why);
   }
 
-  BBTC_TRY(build_block(ctx, g->fwd, d_indptr, d_indices, rows.as<uint32_t>(), n, m, g->cuts, d_cuts.as<uint32_t>(),
-                       nullptr, nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
+  // the forward block CSR waits until something needs it (ensure_fwd): the
+  // fused task rows read only the reversed one
 
   // word-compressed rows (the fused task rows stream these)
   DevBuf wflags, wpos;
@@ -596,17 +624,48 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
                          g->d_wptr, stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), grid));
   }
   // the host needs the tile statistics only now: one read-back for both block CSRs
-  BBTC_TRY(fetch_stats(g->fwd, g->rev, stats.as<uint32_t>(), coloff.as<uint64_t>(), stats_r.as<uint32_t>(),
-                       coloff_r.as<uint64_t>(), s));
+  BBTC_TRY(fetch_stats(ctx, nullptr, g->rev, nullptr, nullptr, stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), s));
   BBTC_CUDA(cudaEventRecord(ev1, s));
   BBTC_CUDA(cudaEventSynchronize(ev1));
   float ms = 0;
   BBTC_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   g->layout_ms = ms;
-  g->device_bytes = (g->fwd.rp_len + g->fwd.col_len + g->rev.rp_len + g->rev.col_len) * sizeof(uint32_t) +
-                    g->rev.col_len * sizeof(uint2) + ((uint64_t)n + 1 + m) * sizeof(uint32_t) + 64 * sizeof(uint64_t) +
-                    m * sizeof(uint2) + ((uint64_t)n + 1) * sizeof(uint32_t) +
-                    (g->fwd.erow_len + g->rev.erow_len) * sizeof(uint32_t);
+  g->device_bytes = block_bytes(g->rev, true) + ((uint64_t)n + 1 + m) * sizeof(uint32_t) + 64 * sizeof(uint64_t) +
+                    m * sizeof(uint2) + ((uint64_t)n + 1) * sizeof(uint32_t);
+  return BBTC_OK;
+}
+
+int ensure_fwd(bbtc_graph* g) {
+  if (g->fwd_built) return BBTC_OK;
+  bbtc_ctx* ctx = g->ctx;
+  cudaStream_t s = ctx->stream;
+  BBTC_CUDA(cudaSetDevice(ctx->device));
+  const uint32_t n = g->n, P = g->P, T = P * P;
+  const uint64_t m = g->m;
+  const int grid = layout_grid(ctx, n, m, P);
+  DevBuf d_cuts, bad, rows, stats, coloff;
+  BBTC_TRY(dalloc(d_cuts, g->cuts.size() * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(bad, sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(rows, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(stats, 4 * T * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(coloff, T * sizeof(uint64_t), s));
+  {
+    uint32_t* h = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageCuts);
+    std::memcpy(h, g->cuts.data(), g->cuts.size() * sizeof(uint32_t));
+    BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, h, g->cuts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  }
+  if (n > 0) {
+    // row id of every edge (the CSR passed validation when it was uploaded)
+    BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
+    k_expand_check<<<grid, 256, 0, s>>>(g->d_indptr, g->d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>());
+    BBTC_CUDA(cudaGetLastError());
+  }
+  BBTC_TRY(build_block(ctx, g->fwd, g->d_indptr, g->d_indices, rows.as<uint32_t>(), n, m, g->cuts,
+                       d_cuts.as<uint32_t>(), nullptr, nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(),
+                       grid));
+  BBTC_TRY(fetch_stats(ctx, nullptr, g->fwd, nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(), s));
+  g->fwd_built = true;
+  g->device_bytes += block_bytes(g->fwd, false);
   return BBTC_OK;
 }
 

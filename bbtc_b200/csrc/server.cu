@@ -3,17 +3,19 @@
 // No counterpart in the reference (it counts one graph per process).  A
 // request is a host CSR + cut vector; its answer is the exact count.
 //
-//   loader threads (each with its own high-priority stream): take a pending
-//     request whose estimated device footprint fits the HBM budget -- the
-//     smallest, or the oldest once it has waited aging_ms -- build its device
-//     block CSR (upload + layout), and queue it on its size class's lane.  A
+//   loader threads: take a pending request whose estimated device footprint
+//     fits the HBM budget -- the smallest, or the oldest once it has waited
+//     aging_ms -- build its device block CSR (upload + layout) on the
+//     loader's stream for its size class (small: highest priority; large:
+//     lowest priority, layout grids capped at 4 blocks per SM), and queue it
+//     on its size class's lane.  A
 //     request that could never fit fails with BBTC_ERR_CAPACITY.  With two or
 //     more loaders the first one takes small requests only.
 //   two launcher threads (lanes), each with its own stream: lane 0 counts
 //     graphs of at most small_edges edges at the highest stream priority,
-//     lane 1 the larger ones with its persistent grid capped below the
-//     occupancy limit, so a small request never waits for a large count to
-//     drain the GPU.  A lane takes every ready graph of its class (up to
+//     lane 1 the larger ones with its persistent blocks kept off small_sms
+//     SMs, so a small request never waits for a large count to drain the
+//     GPU.  A lane takes every ready graph of its class (up to
 //     max_batch), counts them in one persistent launch with one u64 slot per
 //     graph, publishes the counts, frees the graphs, returns their memory to
 //     the budget.  The device memory pool is grown once at creation.
@@ -25,6 +27,7 @@
 // on what shares its launch.
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <chrono>
@@ -87,16 +90,18 @@ namespace {
 
 // One launch lane: a launcher thread with its own stream, result slots and
 // ready queue.  Lane 0 counts the small graphs on a high-priority stream;
-// lane 1 the large ones, with its persistent grid capped so that lane 0's
-// launches (and the loaders' layout kernels) always find free block slots.
+// lane 1 the large ones, its persistent blocks leaving the lowest-numbered
+// SMs free, so that lane 0's launches (and the loaders' layout kernels)
+// always find SMs no large count holds.
 struct Lane {
   bbtc_ctx* ctx = nullptr;
   std::deque<Request*> ready;
   std::condition_variable cv;
   std::thread th;
   uint64_t* d_outs = nullptr;
-  std::vector<uint64_t> h_outs;
+  uint64_t* h_outs = nullptr;  // pinned: the readback waits only for this lane's stream
   uint32_t blocks_per_sm = 0;  // 0: as many as fit
+  uint32_t spare_sms = 0;      // SMs this lane's counts leave free
   uint64_t launches = 0;
 };
 
@@ -106,7 +111,7 @@ struct Lane {
 struct bbtc_server {
   bbtc_server_opts opts{};
   int device = 0;
-  std::vector<bbtc_ctx*> load_ctx;
+  std::vector<bbtc_ctx*> load_ctx;  // two per loader: small requests, large requests
   std::mutex mu;
   std::condition_variable cv_load, cv_done;
   std::deque<bbtc::Request*> pending;
@@ -154,7 +159,7 @@ Request* pick(bbtc_server* s, bool small_only) {
   return r;
 }
 
-void loader_main(bbtc_server* s, bbtc_ctx* ctx, bool small_only) {
+void loader_main(bbtc_server* s, bbtc_ctx* ctx_small, bbtc_ctx* ctx_large, bool small_only) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
@@ -176,6 +181,9 @@ void loader_main(bbtc_server* s, bbtc_ctx* ctx, bool small_only) {
     s->loading++;
     lk.unlock();
     bbtc_graph* g = nullptr;
+    // a large layout runs on a low-priority stream with its grids capped, so
+    // the small ones' kernels are scheduled first and find free SMs
+    bbtc_ctx* ctx = lane_of(s, r) == 0 ? ctx_small : ctx_large;
     const int rc = bbtc_graph_upload(ctx, r->n, r->indptr, r->indices, r->m, r->cuts.data(),
                                      (uint32_t)r->cuts.size() - 1, &g);
     lk.lock();
@@ -228,20 +236,22 @@ void launcher_main(bbtc_server* s, uint32_t lane) {
     bbtc_opts o = s->opts.count;
     o.use_cuda_graph = 0;
     if (L.blocks_per_sm && (!o.blocks_per_sm || o.blocks_per_sm > L.blocks_per_sm)) o.blocks_per_sm = L.blocks_per_sm;
+    if (L.spare_sms) o.spare_sms = L.spare_sms;
     const bool fused = o.kernel == BBTC_KERNEL_FUSED || (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT);
     int rc = BBTC_OK;
     if (!fused) {
       for (size_t i = 0; i < batch.size(); i++) {
+        if (rc == BBTC_OK) rc = ensure_fwd(gs[i]);
         uint32_t nt = 0;
         bbtc_task_list(gs[i]->P, nullptr, 0, &nt);
         tl[i].resize(nt);
         bbtc_task_list(gs[i]->P, tl[i].data(), nt, &nt);
       }
     }
-    rc = count_enqueue(ctx, gs, tl, o, fused, L.d_outs, &plan, false);
+    if (rc == BBTC_OK) rc = count_enqueue(ctx, gs, tl, o, fused, L.d_outs, &plan, false);
     if (rc == BBTC_OK) {
       const cudaError_t e =
-          cudaMemcpyAsync(L.h_outs.data(), L.d_outs, batch.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+          cudaMemcpyAsync(L.h_outs, L.d_outs, batch.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                           ctx->stream);
       const cudaError_t e2 = e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
       if (e2 != cudaSuccess) rc = cuda_fail(e2, "server batch readback");
@@ -313,10 +323,15 @@ void bbtc_server_opts_default(bbtc_server_opts* o) {
   o->large_blocks_per_sm = 0;
   o->aging_ms = 50;
   o->pool_bytes = 0;
+  o->small_sms = 16;
 }
 
 int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** out) {
   if (!out) return fail(BBTC_ERR_ARG, "out is NULL");
+  // one hardware work queue per stream: with the default 8, a small lane's
+  // launch that hashed onto the large lane's queue waited for its count to
+  // finish.  Takes effect only if CUDA is not initialised in the process yet.
+  setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
   *out = nullptr;
   bbtc_server* s = new (std::nothrow) bbtc_server();
   if (!s) return fail(BBTC_ERR_NOMEM, "host allocation failed");
@@ -339,16 +354,18 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
     rc = bbtc_ctx_create(device, &s->lanes[l].ctx);
     if (rc == BBTC_OK) rc = set_stream_priority(s->lanes[l].ctx, l == 0 ? hi : lo);
   }
-  for (uint32_t i = 0; rc == BBTC_OK && i < s->opts.loaders; i++) {
+  for (uint32_t i = 0; rc == BBTC_OK && i < 2 * s->opts.loaders; i++) {
     bbtc_ctx* c = nullptr;
     rc = bbtc_ctx_create(device, &c);
     if (rc == BBTC_OK) s->load_ctx.push_back(c);
-    if (rc == BBTC_OK) rc = set_stream_priority(c, hi);
+    if (rc == BBTC_OK) rc = set_stream_priority(c, i % 2 == 0 ? hi : lo);
+    if (rc == BBTC_OK && i % 2 == 1) c->layout_blocks_per_sm = 4;
   }
   for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
-    if (cudaMalloc(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess) {
+    if (cudaMalloc(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess ||
+        cudaMallocHost(&s->lanes[l].h_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess) {
       cudaGetLastError();
-      rc = fail(BBTC_ERR_NOMEM, "device allocation of the result slots failed");
+      rc = fail(BBTC_ERR_NOMEM, "allocation of the result slots failed");
     }
   }
   if (rc != BBTC_OK) {
@@ -356,22 +373,46 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
     for (auto& L : s->lanes) {
       if (L.ctx) bbtc_ctx_destroy(L.ctx);
       if (L.d_outs) cudaFree(L.d_outs);
+      if (L.h_outs) cudaFreeHost(L.h_outs);
     }
     delete s;
     return rc;
   }
   {
-    // the large lane leaves a third of the occupancy target (at least one
-    // block per SM) to the small lane
-    const uint32_t occ = s->opts.count.occupancy >= 8 ? 8 : (s->opts.count.occupancy >= 6 ? 6 : 4);
-    s->lanes[1].blocks_per_sm =
-        s->opts.large_blocks_per_sm ? s->opts.large_blocks_per_sm : occ - std::max<uint32_t>(1, occ / 3);
+    // the large lane's counts leave small_sms SMs to the small requests, and
+    // use at most 4 blocks per SM: a persistent launch ends only once its
+    // last block has been scheduled, and blocks that do not fit beside the
+    // high-priority small work at launch waited behind it for hundreds of ms
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    s->lanes[1].blocks_per_sm = s->opts.large_blocks_per_sm ? s->opts.large_blocks_per_sm : 4;
+    s->lanes[1].spare_sms = std::min<uint32_t>(s->opts.small_sms, (uint32_t)std::max(sms / 2, 1));
   }
   {
-    // grow the device's memory pool once, now: a pool that grows while loads
-    // and counts run stalled every loader for hundreds of milliseconds
+    // memory freed on one stream is handed to another only once the free has
+    // completed: with reuse that follows event dependencies, a small load
+    // whose allocation took blocks a large load had just freed waited behind
+    // that load (and the counts ahead of it) for tens of milliseconds
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      int off = 0;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolReuseFollowEventDependencies, &off);
+      cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &off);
+    }
+    cudaGetLastError();
+  }
+  {
+    // grow the device's memory pool once, now, to what the admission budget
+    // can hold: a pool that grows while loads and counts run stalled every
+    // loader for hundreds of milliseconds (up to 1.5 s when it grew by GBs)
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      free_b = 0;
+    }
+    const uint64_t cap = free_b > (8ull << 30) ? free_b - (8ull << 30) : free_b / 2;
     const uint64_t want =
-        s->opts.pool_bytes ? s->opts.pool_bytes : std::min<uint64_t>(s->opts.hbm_budget, 48ull << 30);
+        std::min<uint64_t>(s->opts.pool_bytes ? s->opts.pool_bytes : s->opts.hbm_budget + s->opts.hbm_budget / 10, cap);
     cudaStream_t st = s->lanes[0].ctx->stream;
     void* p = nullptr;
     if (cudaMallocAsync(&p, want, st) == cudaSuccess) {
@@ -381,10 +422,9 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
       cudaGetLastError();  // not fatal: the pool grows on demand instead
     }
   }
-  for (auto& L : s->lanes) L.h_outs.assign(s->opts.max_batch, 0);
   // with two or more loaders, the first takes small requests only
-  for (size_t i = 0; i < s->load_ctx.size(); i++)
-    s->loaders.emplace_back(loader_main, s, s->load_ctx[i], i == 0 && s->load_ctx.size() > 1);
+  for (size_t i = 0; i < s->opts.loaders; i++)
+    s->loaders.emplace_back(loader_main, s, s->load_ctx[2 * i], s->load_ctx[2 * i + 1], i == 0 && s->opts.loaders > 1);
   for (uint32_t l = 0; l < 2; l++) s->lanes[l].th = std::thread(launcher_main, s, l);
   *out = s;
   return BBTC_OK;
@@ -415,9 +455,16 @@ int bbtc_server_destroy(bbtc_server* s) {
   for (auto& L : s->lanes) {
     cudaStreamSynchronize(L.ctx->stream);
     cudaFree(L.d_outs);
+    cudaFreeHost(L.h_outs);
   }
   for (auto* c : s->load_ctx) bbtc_ctx_destroy(c);
   for (auto& L : s->lanes) bbtc_ctx_destroy(L.ctx);
+  {
+    // hand the pool's unused memory back (it was grown to the budget at creation)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
+  }
   delete s;
   return BBTC_OK;
 }

@@ -35,6 +35,10 @@ import time
 
 import numpy as np
 
+# one hardware work queue per stream (the serving mode runs ten or more);
+# read when the process initialises CUDA, so set before torch is imported
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
