@@ -23,7 +23,7 @@ BIN = os.path.join(HERE, "bin")
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("BBTC_CXX", shutil.which("g++") or "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["api.cu", "layout.cu", "count.cu", "server.cu", "prep.cu"]
+CUDA_SOURCES = ["api.cu", "layout.cu", "count.cu", "server.cu", "prep.cu", "partition_dev.cu"]
 HOST_SOURCES = ["graphgen.cpp", "partition.cpp", "graph_io.cpp"]
 
 
@@ -40,7 +40,7 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 
 def _deps(names: list[str]) -> list[str]:
-    extra = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    extra = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh", ".hpp"))]
     return [os.path.join(CSRC, n) for n in names] + extra + [os.path.join(ROOT, "include", "bbtc_gpu.h")]
 
 

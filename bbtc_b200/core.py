@@ -487,6 +487,7 @@ def _prep_lib():
         "bbtc_rmat_device": [vp, c.c_int, c.c_int, c.c_double, c.c_double, c.c_double, c.c_uint64, vp, vp],
         "bbtc_orient_device": [vp, c.c_uint32, vp, vp, c.c_uint64, c.POINTER(CsrDev)],
         "bbtc_csr_dev_free": [vp, c.POINTER(CsrDev)],
+        "bbtc_cuts_device": [vp, c.c_int, c.c_uint32, vp, vp, c.c_uint64, c.c_uint32, c.c_uint64, vp],
     }.items():
         f = getattr(L, name)
         f.argtypes = args
@@ -499,6 +500,16 @@ def rmat_device(ctx: Context, scale: int, edge_factor: int, d_src: int, d_dst: i
                 a: float = 0.57, b: float = 0.19, cc: float = 0.19) -> None:
     """Fill device buffers (edge_factor << scale entries each) with R-MAT pairs."""
     check(_prep_lib().bbtc_rmat_device(ctx.handle, scale, edge_factor, a, b, cc, seed, d_src, d_dst))
+
+
+def cuts_device(ctx: Context, kind: str | int, n: int, d_indptr: int, d_indices: int, m: int, P: int,
+                seed: int = 1091467301) -> np.ndarray:
+    """Cut vector of a device CSR computed on the GPU (bbtc_cuts_device): the
+    same cuts as graphs.cuts on the same CSR.  kind: "uni", "n1d" or "pal"."""
+    k = {"uni": 0, "n1d": 1, "pal": 2}[kind] if isinstance(kind, str) else int(kind)
+    out = np.zeros(P + 1, dtype=np.uint32)
+    check(_prep_lib().bbtc_cuts_device(ctx.handle, k, n, d_indptr, d_indices, m, P, seed, out.ctypes.data))
+    return out
 
 
 class DeviceCSR:
@@ -527,6 +538,10 @@ class DeviceCSR:
 
     def graph(self, cuts) -> Graph:
         return Graph.upload_device(self.ctx, self.n, self.indptr_ptr, self.indices_ptr, self.m, cuts)
+
+    def cuts(self, P: int, kind: str = "pal", seed: int = 1091467301) -> np.ndarray:
+        """Cut vector computed on the GPU (bbtc_cuts_device)."""
+        return cuts_device(self.ctx, kind, self.n, self.indptr_ptr, self.indices_ptr, self.m, P, seed)
 
     def free(self) -> None:
         if self._c.indptr:

@@ -124,6 +124,34 @@ struct bbtc_ctx {
   char* h_stage = nullptr;
 };
 
+namespace bbtc {
+
+// Stream-ordered device buffer (freed on the stream it was allocated on).
+struct DevBuf {
+  void* p = nullptr;
+  cudaStream_t s = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, s);
+  }
+  template <class T>
+  T* as() { return static_cast<T*>(p); }
+};
+
+inline int dalloc(DevBuf& b, size_t bytes, cudaStream_t s) {
+  b.s = s;
+  cudaError_t e = cudaMallocAsync(&b.p, bytes > 16 ? bytes : 16, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    return fail(BBTC_ERR_NOMEM, std::string("device allocation of ") + std::to_string(bytes) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+  }
+  return BBTC_OK;
+}
+
 // Regions of bbtc_ctx::h_stage (one graph build or count at a time per context).
 constexpr size_t kStageBytes = 1u << 20;
 constexpr size_t kStageCuts = 0;          // cut vector, <= (64 + 1) x 4 bytes
@@ -131,6 +159,8 @@ constexpr size_t kStageBad = 3072;        // validation flags
 constexpr size_t kStageOff[2] = {4096, 40960};  // per block CSR: tile + part row offsets (<= 33,288 bytes)
 constexpr size_t kStageStats = 81920;     // tile statistics of both block CSRs (<= 163,840 bytes)
 constexpr size_t kStageOut = 262144;      // counts read back (<= 98,304 of them)
+
+}  // namespace bbtc
 
 struct bbtc_graph {
   bbtc_ctx* ctx = nullptr;

@@ -308,29 +308,6 @@ __global__ void k_gather(const uint32_t* __restrict__ src, const uint32_t* __res
 
 inline uint64_t align4(uint64_t x) { return (x + 3) & ~3ull; }
 
-// Stream-ordered device buffer (freed on the context stream).
-struct DevBuf {
-  void* p = nullptr;
-  cudaStream_t s = nullptr;
-  ~DevBuf() {
-    if (p) cudaFreeAsync(p, s);
-  }
-  template <class T>
-  T* as() { return static_cast<T*>(p); }
-};
-
-int dalloc(DevBuf& b, size_t bytes, cudaStream_t s) {
-  b.s = s;
-  cudaError_t e = cudaMallocAsync(&b.p, std::max<size_t>(bytes, 16), s);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    b.p = nullptr;
-    return fail(BBTC_ERR_NOMEM, std::string("device allocation of ") + std::to_string(bytes) +
-                                    " bytes failed: " + cudaGetErrorString(e));
-  }
-  return BBTC_OK;
-}
-
 // Build one block CSR (forward or reversed) from a CSR in device memory whose
 // per-edge row ids are `rows`.  With `eids` the reversed build also writes the
 // forward-edge records.  The tile statistics land in `st` (device, 4*P*P words)

@@ -108,7 +108,7 @@ def from_pairs(n: int, src, dst, name: str = "pairs") -> OrientedCSR:
     return _take(h, name, dict(kind="pairs"))
 
 
-PARTITIONERS = {"uni": 0, "n1d": 1, "pal": 2}
+PARTITIONERS = {"uni": 0, "n1d": 1, "pal": 2, "pal-bisect": 3}  # pal-bisect: same cuts as pal, slower probe
 PAL_SEED = 1091467301  # the sampling seed the reference passes (include/utils/utils.hpp:272)
 
 

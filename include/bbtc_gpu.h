@@ -215,12 +215,23 @@ int bbtc_orient_device(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_src, const u
                        bbtc_csr_dev* out);
 int bbtc_csr_dev_free(bbtc_ctx* ctx, bbtc_csr_dev* csr);
 
+/* Cut vector (P + 1 entries, host memory) of a CSR in device memory: the
+ * partitioner on the GPU.  Replaces the host-side SARMA call of the
+ * reference (include/utils/utils.hpp:271-288) for graphs that live on the
+ * device.  kind: 0 = uni, 1 = n1d, 2 = pal (seed: the pal sampling seed, the
+ * reference passes 1091467301).  Gives the same cuts as the host library's
+ * bbtcp_cuts on the same CSR.  Synchronises the context's stream. */
+int bbtc_cuts_device(bbtc_ctx* ctx, int kind, uint32_t n, const uint32_t* d_indptr, const uint32_t* d_indices,
+                     uint64_t m, uint32_t P, uint64_t seed, uint32_t* cuts);
+
 /* ---- request server: continuous batching ----------------------------------
  * No counterpart in the reference (one graph per process).  Loader threads
  * build each submitted graph's device block CSR on their own streams,
- * admitting requests in arrival order while their estimated device footprint
- * fits hbm_budget; one launcher thread counts every ready graph in a single
- * persistent launch (one u64 slot per graph), publishes the counts and frees
+ * admitting requests (smallest first, oldest first once they have waited
+ * aging_ms) while their estimated device footprint fits hbm_budget; two
+ * launch lanes (small graphs / large graphs) each count every ready graph of
+ * their class in a single persistent launch (one u64 slot per graph),
+ * publish the counts and free
  * the graphs.  Requests that arrive while a launch runs are loaded meanwhile
  * and join the next launch.  All server calls are thread-safe.  The caller's
  * indptr / indices must stay valid until the request finishes (pinned host

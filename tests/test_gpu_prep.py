@@ -60,3 +60,21 @@ def test_orient_device_cleans_pairs(ctx):
     assert g.count() == oracle.count(host.n, host.indptr, host.indices, cuts)
     g.free()
     dev.free()
+
+
+@pytest.mark.parametrize("make", [lambda: graphs.rmat(8, 8, seed=1), lambda: graphs.rmat(16, 16, seed=2),
+                                  lambda: graphs.rgg(1 << 14, seed=4),
+                                  lambda: graphs.chung_lu(1 << 15, seed=5, max_deg=3000)])
+def test_cuts_on_device_equal_host(ctx, make):
+    """bbtc_cuts_device (the partitioner on the GPU) gives the host partitioners'
+    cuts on the same CSR, for every kind and several stripe counts."""
+    torch = pytest.importorskip("torch")
+    g = make()
+    ip = torch.from_numpy(g.indptr.view(np.int32)).cuda()
+    ix = torch.from_numpy(g.indices.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    for kind in ("uni", "n1d", "pal"):
+        for P in (1, 2, 5, 16, 64):
+            got = core.cuts_device(ctx, kind, g.n, ip.data_ptr(), ix.data_ptr(), g.m, P)
+            want = graphs.cuts(g, P, kind)
+            assert np.array_equal(got, want), (kind, P, got, want)

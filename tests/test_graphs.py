@@ -66,3 +66,14 @@ def test_algorithmic_bytes():
     rows = np.repeat(np.arange(g.n), d)
     want = 4 * g.m + 4 * int((d[rows] + d[g.indices]).sum())
     assert g.algorithmic_bytes() == want
+
+
+@pytest.mark.parametrize("make", [lambda: graphs.rmat(8, 16, seed=1), lambda: graphs.rmat(13, 16, seed=2),
+                                  lambda: graphs.rmat(16, 8, seed=3), lambda: graphs.rgg(1 << 13, seed=4),
+                                  lambda: graphs.chung_lu(1 << 14, seed=5, max_deg=1500)])
+def test_pal_sweep_probe_equals_bisection(make):
+    """The sweep probe (default pal) finds the same cut positions as the
+    bisection probe it replaced, for every stripe count."""
+    g = make()
+    for P in (1, 2, 3, 7, 16, 33, 64):
+        assert np.array_equal(graphs.cuts(g, P, "pal"), graphs.cuts(g, P, "pal-bisect")), P
