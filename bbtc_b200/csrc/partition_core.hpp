@@ -7,9 +7,10 @@
 //  * pal_cuts_bisect: for each new cut, a bisection over the rows, each step
 //    recounting the tiles the cut fixes (the first implementation);
 //  * pal_from_sample: for each new cut, the sampled nonzeros that the cut
-//    can fix are sorted by the smallest cut position that includes them and
-//    swept once, so the largest position whose tiles stay within the bound is
-//    found without recounting.  The tile loads only grow with the position,
+//    can fix are read in order of the smallest cut position that includes
+//    them (a merge of the row-sorted and the column-sorted sample) until a
+//    tile exceeds the bound, so the largest position whose tiles stay within
+//    it is found without recounting.  The tile loads only grow with the position,
 //    which makes "largest feasible position" well defined and equal for both.
 #pragma once
 #include <algorithm>
@@ -240,9 +241,16 @@ struct SortedSample {
 
 // Largest m in [p.back(), R] whose new stripe [p.back(), m) keeps every tile
 // it fixes within L (see new_stripe_maxload for the tiles).
+//
+// A sampled nonzero (r, c) is counted from position m = t on, its threshold:
+//  * row stripe tile (r >= lo, column stripe of c): t = max(r, c) + 1;
+//  * column stripe tile (r < lo, lo <= c): t = c + 1.
+// Those with c <= r come in threshold order along the row-sorted sample;
+// the others (c > r, or r < lo) along the column-sorted one.  The two
+// streams are merged by threshold and stopped at the first threshold whose
+// nonzeros push a tile above L: only the nonzeros below the answer are read.
 uint32_t pal_next_cut(const SortedSample& s, const std::vector<uint32_t>& p, uint32_t R, uint64_t L,
-                      std::vector<std::pair<uint32_t, uint32_t>>& ev, std::vector<uint64_t>& ca,
-                      std::vector<uint64_t>& cb) {
+                      std::vector<uint64_t>& ca, std::vector<uint64_t>& cb) {
   const uint32_t lo = p.back();
   if (R <= lo) return lo;
   const size_t parts = p.size();
@@ -250,37 +258,38 @@ uint32_t pal_next_cut(const SortedSample& s, const std::vector<uint32_t>& p, uin
     if (x >= lo) return (uint32_t)(parts - 1);
     return (uint32_t)(std::upper_bound(p.begin(), p.end(), x) - p.begin()) - 1;
   };
-  // events: (smallest m that counts the nonzero, key); key < parts: row-stripe
-  // tile of column stripe `key`; key >= parts: column-stripe tile of row stripe key - parts
-  ev.clear();
-  {
-    const size_t a = std::lower_bound(s.row.begin(), s.row.end(), lo) - s.row.begin();
-    const size_t b = std::lower_bound(s.row.begin(), s.row.end(), R) - s.row.begin();
-    for (size_t t = a; t < b; t++) {
-      const uint32_t c = s.col[t];
-      if (c >= R) continue;
-      ev.emplace_back(std::max(s.row[t], c) + 1, stripe_of(c));
-    }
-  }
-  {
-    const size_t a = std::lower_bound(s.ccol.begin(), s.ccol.end(), lo) - s.ccol.begin();
-    const size_t b = std::lower_bound(s.ccol.begin(), s.ccol.end(), R) - s.ccol.begin();
-    for (size_t t = a; t < b; t++) {
-      const uint32_t r = s.crow[t];
-      if (r >= lo) continue;
-      ev.emplace_back(s.ccol[t] + 1, (uint32_t)parts + stripe_of(r));
-    }
-  }
-  std::sort(ev.begin(), ev.end());
   ca.assign(parts, 0);
   cb.assign(parts, 0);
-  for (size_t t = 0; t < ev.size();) {
-    const uint32_t m = ev[t].first;
+  // stream 1: row-sorted, rows [lo, R), entries with c <= r (threshold r + 1)
+  size_t i = std::lower_bound(s.row.begin(), s.row.end(), lo) - s.row.begin();
+  const size_t i_end = std::lower_bound(s.row.begin(), s.row.end(), R) - s.row.begin();
+  // stream 2: column-sorted, columns [lo, R), entries with r < lo or lo <= r < c (threshold c + 1)
+  size_t j = std::lower_bound(s.ccol.begin(), s.ccol.end(), lo) - s.ccol.begin();
+  const size_t j_end = std::lower_bound(s.ccol.begin(), s.ccol.end(), R) - s.ccol.begin();
+  auto skip1 = [&] {
+    while (i < i_end && s.col[i] > s.row[i]) i++;
+  };
+  auto skip2 = [&] {
+    while (j < j_end && s.crow[j] >= lo && s.crow[j] >= s.ccol[j]) j++;
+  };
+  skip1();
+  skip2();
+  while (i < i_end || j < j_end) {
+    const uint32_t t1 = i < i_end ? s.row[i] + 1 : 0xffffffffu;
+    const uint32_t t2 = j < j_end ? s.ccol[j] + 1 : 0xffffffffu;
+    const uint32_t m = std::min(t1, t2);
     bool over = false;
-    for (; t < ev.size() && ev[t].first == m; t++) {
-      const uint32_t k = ev[t].second;
-      uint64_t& c = k < parts ? ca[k] : cb[k - parts];
+    while (i < i_end && s.row[i] + 1 == m) {
+      if (++ca[stripe_of(s.col[i])] > L) over = true;
+      i++;
+      skip1();
+    }
+    while (j < j_end && s.ccol[j] + 1 == m) {
+      const uint32_t r = s.crow[j];
+      uint64_t& c = r < lo ? cb[stripe_of(r)] : ca[parts - 1];  // r < lo: column stripe tile; else diagonal
       if (++c > L) over = true;
+      j++;
+      skip2();
     }
     if (over) return m - 1;  // m counts a tile above L; every smaller position is within it
   }
@@ -289,10 +298,9 @@ uint32_t pal_next_cut(const SortedSample& s, const std::vector<uint32_t>& p, uin
 
 std::vector<uint32_t> pal_probe_sorted(const SortedSample& s, uint32_t P, uint64_t L, const std::vector<uint32_t>& UB) {
   std::vector<uint32_t> p{0};
-  std::vector<std::pair<uint32_t, uint32_t>> ev;
   std::vector<uint64_t> ca, cb;
   while (p.size() < (size_t)P + 1) {
-    const uint32_t l = pal_next_cut(s, p, UB[p.size()], L, ev, ca, cb);
+    const uint32_t l = pal_next_cut(s, p, UB[p.size()], L, ca, cb);
     if (l == p.back()) {
       while (p.size() < (size_t)P + 1) p.push_back(p.back());
       break;
