@@ -488,8 +488,10 @@ struct FusedFrame {
   const uint32_t* gp;    // oriented CSR
   const uint32_t* gi;
   const uint2* gw;       // word-compressed rows
+  const uint32_t* wp;    // their row pointers
   uint32_t H, e1, b, ee; // rows, unit end, current row, end of the current row's entries
   uint32_t pivot_base, ps, pd, base, words, rlen, kind, slot;
+  uint32_t ws, wn;       // the pivot row's word pairs
 };
 static_assert(sizeof(FusedFrame) <= (kSegWords - kFrameOffset) * sizeof(uint32_t), "frame does not fit");
 
@@ -554,6 +556,34 @@ __device__ __forceinline__ void fused_build(const uint32_t* __restrict__ prow, u
   }
 }
 
+// Bitmap of a pivot row from its word pairs: one plain store per 32-id word
+// (a row holds each word once), where setting the bits id by id took one
+// shared-memory atomic per id, serialised on the words that several ids
+// share.  Split kind: only the words of its window (w >= base_w).
+template <uint32_t KIND>
+__device__ __forceinline__ void fused_build_words(const uint2* __restrict__ pw, uint32_t wn, uint32_t base_w,
+                                                  uint32_t* bm, uint32_t lane) {
+  for (uint32_t i = lane; i < wn; i += 32) {
+    const uint2 w = pw[i];
+    if (KIND == kPivotBitmap || w.x >= base_w) bm[w.x - base_w] = w.y;
+  }
+}
+
+template <uint32_t KIND>
+__device__ __forceinline__ void fused_clear_words(const uint2* __restrict__ pw, uint32_t wn, uint32_t base_w,
+                                                  uint32_t words, uint32_t* bm, uint32_t lane) {
+  // up to 512 words (bitmap kind), or as many as the row has pairs, are
+  // cleared as a range (stores only); otherwise the row's words, read again
+  if ((KIND == kPivotBitmap && words <= 512) || wn >= words) {
+    for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
+  } else {
+    for (uint32_t i = lane; i < wn; i += 32) {
+      const uint32_t x = pw[i].x;
+      if (KIND == kPivotBitmap || x >= base_w) bm[x - base_w] = 0;
+    }
+  }
+}
+
 template <uint32_t KIND>
 __device__ __forceinline__ void fused_clear(const uint32_t* __restrict__ prow, uint32_t pd, uint32_t base,
                                             uint32_t words, uint32_t rlen, uint32_t* bm, uint32_t* res,
@@ -604,7 +634,9 @@ __device__ __noinline__ uint32_t fused_wide(volatile FusedFrame* fr, uint32_t ki
                                             uint32_t bm_words, uint32_t lane) {
   uint32_t* res = bm + fr->words + 1;
   if (kind == kPivotSplit) {
-    fused_build<kPivotSplit>(prow, fr->pd, fr->base, fr->rlen, bm, res, lane);
+    const uint32_t rlen = fr->rlen;
+    for (uint32_t i = lane; i < rlen; i += 32) res[i] = prow[i];
+    fused_build_words<kPivotSplit>((const uint2*)fr->gw + fr->ws, fr->wn, fr->base >> 5, bm, lane);
     __syncwarp();
     return fused_probe<kPivotSplit>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
   }
@@ -651,6 +683,7 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
       fr->gp = tk->g_indptr;
       fr->gi = tk->g_indices;
       fr->gw = tk->g_words;
+      fr->wp = tk->g_wptr;
       fr->H = tk->rows.H;
       fr->e1 = nnz - e0 > tk->unit_edges ? e0 + tk->unit_edges : nnz;
       fr->b = tk->rows.erow[e0 >> 5];  // units start at multiples of 32 entries
@@ -670,10 +703,14 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
         const uint32_t v = fr->pivot_base + b;
         const uint32_t ps = fr->gp[v];
         const uint32_t pd = fr->gp[v + 1] - ps;
+        const uint32_t ws = fr->wp[v];
+        const uint32_t wn = fr->wp[v + 1] - ws;
         fused_choose(fr, fr->gi + ps, pd, bm_words, lane);
         if (lane == 0) {
           fr->ee = ee;
           fr->ps = ps;
+          fr->ws = ws;
+          fr->wn = wn;
         }
         __syncwarp();
       }
@@ -684,7 +721,7 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
         uint32_t* res = bm + fr->words + 1;
         switch (kind) {
           case kPivotBitmap:
-            fused_build<kPivotBitmap>(prow, fr->pd, fr->base, 0, bm, res, lane);
+            fused_build_words<kPivotBitmap>((const uint2*)fr->gw + fr->ws, fr->wn, fr->base >> 5, bm, lane);
             __syncwarp();
             acc += fused_probe<kPivotBitmap>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
             break;
@@ -696,11 +733,15 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
         {
           const uint32_t* prow2 = fr->gi + fr->ps;
           uint32_t* res2 = bm + fr->words + 1;
+          const uint2* pw = (const uint2*)fr->gw + fr->ws;
           switch (fr->kind) {
-            case kPivotBitmap: fused_clear<kPivotBitmap>(prow2, fr->pd, fr->base, fr->words, 0, bm, res2, lane); break;
-            case kPivotSplit:
-              fused_clear<kPivotSplit>(prow2, fr->pd, fr->base, fr->words, fr->rlen, bm, res2, lane);
+            case kPivotBitmap: fused_clear_words<kPivotBitmap>(pw, fr->wn, fr->base >> 5, fr->words, bm, lane); break;
+            case kPivotSplit: {
+              fused_clear_words<kPivotSplit>(pw, fr->wn, fr->base >> 5, fr->words, bm, lane);
+              const uint32_t rlen = fr->rlen;
+              for (uint32_t i = lane; i < rlen; i += 32) res2[i] = 0;
               break;
+            }
             case kPivotList: fused_clear<kPivotList>(prow2, fr->pd, 0, 0, 0, bm, res2, lane); break;
             default: break;
           }
@@ -799,6 +840,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
           d.g_indptr = g->d_indptr;
           d.g_indices = g->d_indices;
           d.g_words = reinterpret_cast<const uint2*>(g->d_words);
+          d.g_wptr = g->d_wptr;
           d.pivot_base = g->cuts[j];
           add(d, 0.5 * part_row_len(g, i));
           if (!o.unit_work) list.back().unit_edges = 0;  // set below from the request's size

@@ -67,6 +67,7 @@ struct DevTask {
   const uint32_t* g_indptr;   // fused task rows: the resident oriented CSR
   const uint32_t* g_indices;
   const uint2* g_words;       // fused: word-compressed rows
+  const uint32_t* g_wptr;     // fused: their row pointers (n + 1)
   uint32_t pivot_base;        // fused: first vertex id of part j
   uint32_t kind;
   uint32_t unit_edges;  // entries of `rows` per work unit
