@@ -46,8 +46,7 @@ class Task(c.Structure):
 class Opts(c.Structure):
     _fields_ = [("mode", c.c_int), ("kernel", c.c_int), ("bitmap_words", c.c_uint32),
                 ("warps_per_block", c.c_uint32), ("unit_work", c.c_uint32), ("blocks_per_sm", c.c_uint32),
-                ("use_cuda_graph", c.c_int), ("sort_tasks", c.c_int), ("occupancy", c.c_uint32),
-                ("spare_sms", c.c_uint32)]
+                ("use_cuda_graph", c.c_int), ("sort_tasks", c.c_int), ("occupancy", c.c_uint32)]
 
 
 class GraphInfo(c.Structure):
@@ -109,7 +108,7 @@ def check(rc: int) -> None:
 
 def options(mode: str | int = "persistent", kernel: str | int = "auto", bitmap_words: int = 0,
             warps_per_block: int = 0, unit_work: int = 0, blocks_per_sm: int = 0, cuda_graph: bool = True,
-            sort_tasks: bool = True, occupancy: int = 0, spare_sms: int = 0) -> Opts:
+            sort_tasks: bool = True, occupancy: int = 0) -> Opts:
     o = Opts()
     lib().bbtc_opts_default(c.byref(o))
     o.mode = MODES[mode] if isinstance(mode, str) else int(mode)
@@ -125,7 +124,6 @@ def options(mode: str | int = "persistent", kernel: str | int = "auto", bitmap_w
     o.sort_tasks = 1 if sort_tasks else 0
     if occupancy:
         o.occupancy = occupancy
-    o.spare_sms = spare_sms
     return o
 
 
@@ -354,7 +352,7 @@ class ServerOpts(c.Structure):
     _fields_ = [("hbm_budget", c.c_uint64), ("max_batch", c.c_uint32), ("max_requests", c.c_uint32),
                 ("loaders", c.c_uint32), ("reserved", c.c_uint32), ("count", Opts),
                 ("small_edges", c.c_uint64), ("large_blocks_per_sm", c.c_uint32), ("aging_ms", c.c_uint32),
-                ("pool_bytes", c.c_uint64), ("small_sms", c.c_uint32), ("reserved3", c.c_uint32)]
+                ("pool_bytes", c.c_uint64)]
 
 
 class RequestInfo(c.Structure):
@@ -397,7 +395,7 @@ class Server:
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch: int = 0, loaders: int = 0,
                  opts: Opts | None = None, small_edges: int = 0, large_blocks_per_sm: int = 0,
-                 aging_ms: int | None = None, pool_bytes: int = 0, small_sms: int | None = None):
+                 aging_ms: int | None = None, pool_bytes: int = 0):
         L = _server_lib()
         so = ServerOpts()
         L.bbtc_server_opts_default(c.byref(so))
@@ -417,8 +415,6 @@ class Server:
             so.aging_ms = aging_ms
         if pool_bytes:
             so.pool_bytes = pool_bytes
-        if small_sms is not None:
-            so.small_sms = small_sms
         self._h = c.c_void_p()
         check(L.bbtc_server_create(device, c.byref(so), c.byref(self._h)))
         self._keep: dict[int, tuple] = {}

@@ -405,12 +405,6 @@ __device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_
   return acc;
 }
 
-__device__ __forceinline__ uint32_t sm_id() {
-  uint32_t id;
-  asm volatile("mov.u32 %0, %%smid;" : "=r"(id));
-  return id;
-}
-
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(FULL, v, d);
@@ -430,10 +424,8 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_count_queue(const DevTask* __restrict__ tasks,
                                                         const uint32_t* __restrict__ prefix, uint32_t ntasks,
                                                         uint32_t total_units, uint32_t* __restrict__ head,
-                                                        unsigned long long* __restrict__ outs, uint32_t bm_words,
-                                                        uint32_t spare_sms) {
+                                                        unsigned long long* __restrict__ outs, uint32_t bm_words) {
   extern __shared__ __align__(16) uint32_t sh[];
-  if (spare_sms && blockIdx.x != 0 && sm_id() < spare_sms) return;  // block 0 stays: the queue always drains
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
   uint32_t* sstart = bm + bm_words;
@@ -653,10 +645,8 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __restrict__ tasks,
                                                         const uint32_t* __restrict__ prefix, uint32_t ntasks,
                                                         uint32_t total_units, uint32_t* __restrict__ head,
-                                                        unsigned long long* __restrict__ outs, uint32_t bm_words,
-                                                        uint32_t spare_sms) {
+                                                        unsigned long long* __restrict__ outs, uint32_t bm_words) {
   extern __shared__ __align__(16) uint32_t sh[];
-  if (spare_sms && blockIdx.x != 0 && sm_id() < spare_sms) return;  // block 0 stays: the queue always drains
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
   uint32_t* sstart = bm + bm_words;
@@ -958,7 +948,7 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ctx->sms * per_sm, want));
     BBTC_CUDA(cudaMemsetAsync(ctx->d_unit_counter, 0, sizeof(uint32_t), s));
     kern<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units, ctx->d_unit_counter,
-                                    outs, bmw, o.spare_sms);
+                                    outs, bmw);
     BBTC_CUDA(cudaGetLastError());
     plan->launches = 1;
   }

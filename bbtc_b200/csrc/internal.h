@@ -117,6 +117,7 @@ struct bbtc_ctx {
   uint32_t* d_unit_counter = nullptr;  // persistent-queue head (one word per launch slot)
   size_t smem_set = 0;                 // dynamic shared memory the count kernels are opted in to
   uint32_t layout_blocks_per_sm = 8;   // grid cap of the layout kernels (256 threads a block)
+  uint32_t upload_window = 0;          // host uploads: pieces in flight at most (0 = all at once)
   // Page-locked staging for the small control copies (cut vectors, tile
   // offsets and statistics, counts).  A copy to or from pageable memory is
   // staged by the driver through buffers every thread shares, so one that

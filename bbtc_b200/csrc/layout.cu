@@ -497,11 +497,32 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     // host copies in 8 MiB pieces: a copy engine runs one copy at a time, and
     // another stream's small upload then waits behind one piece, not behind
     // a whole large graph (273 MB at R-MAT s22: about 5 ms)
+    // With an upload window (the server's large requests) at most that many
+    // pieces are queued at once, so the copy engines' queues never hold a
+    // large graph's whole upload ahead of another stream's small one.
+    const uint32_t window = host ? ctx->upload_window : 0;
+    cudaEvent_t evs[8] = {};
+    struct EvRing {
+      cudaEvent_t* e;
+      ~EvRing() {
+        for (int i = 0; i < 8; i++)
+          if (e[i]) cudaEventDestroy(e[i]);
+      }
+    } ring{evs};
+    uint32_t issued = 0;
     auto copy = [&](void* dst, const void* src, size_t bytes) -> int {
       const size_t piece = host ? (size_t)8 << 20 : bytes;
-      for (size_t o = 0; o < bytes; o += piece)
+      for (size_t o = 0; o < bytes; o += piece) {
+        if (window) {
+          cudaEvent_t& ev = evs[issued % std::min<uint32_t>(window, 8)];
+          if (ev) BBTC_CUDA(cudaEventSynchronize(ev));
+          else BBTC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        }
         BBTC_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o,
                                   std::min(piece, bytes - o), kind, s));
+        if (window) BBTC_CUDA(cudaEventRecord(evs[issued % std::min<uint32_t>(window, 8)], s));
+        issued++;
+      }
       return BBTC_OK;
     };
     BBTC_TRY(copy(g->d_indptr, in_indptr, ((size_t)n + 1) * sizeof(uint32_t)));

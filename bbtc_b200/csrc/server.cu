@@ -7,18 +7,19 @@
 //     fits the HBM budget -- the smallest, or the oldest once it has waited
 //     aging_ms -- build its device block CSR (upload + layout) on the
 //     loader's stream for its size class (small: highest priority; large:
-//     lowest priority, layout grids capped at 4 blocks per SM), and queue it
-//     on its size class's lane.  A
-//     request that could never fit fails with BBTC_ERR_CAPACITY.  With two or
-//     more loaders the first one takes small requests only.
-//   two launcher threads (lanes), each with its own stream: lane 0 counts
-//     graphs of at most small_edges edges at the highest stream priority,
-//     lane 1 the larger ones with its persistent blocks kept off small_sms
-//     SMs, so a small request never waits for a large count to drain the
-//     GPU.  A lane takes every ready graph of its class (up to
-//     max_batch), counts them in one persistent launch with one u64 slot per
-//     graph, publishes the counts, frees the graphs, returns their memory to
-//     the budget.  The device memory pool is grown once at creation.
+//     lowest priority, layout grids capped at 2 blocks per SM, at most two
+//     8 MiB upload pieces queued at a time), and queue it on its size
+//     class's lane.  A request that could never fit fails with
+//     BBTC_ERR_CAPACITY.  With two or more loaders the first one takes small
+//     requests only.
+//   two launcher threads (lanes), each with its own highest-priority stream:
+//     lane 0 counts graphs of at most small_edges edges, lane 1 the larger
+//     ones with at most 3 blocks per SM, so a small request never waits for
+//     a large count to drain the GPU.  A lane takes every ready graph of its
+//     class (up to max_batch), counts them in one persistent launch with one
+//     u64 slot per graph, publishes the counts, frees the graphs, returns
+//     their memory to the budget.  The device memory pool is grown once at
+//     creation.
 //
 // So requests that arrive while a launch is on the GPU are uploaded and laid
 // out on the loader streams at the same time, and join the next launch; the
@@ -101,7 +102,6 @@ struct Lane {
   uint64_t* d_outs = nullptr;
   uint64_t* h_outs = nullptr;  // pinned: the readback waits only for this lane's stream
   uint32_t blocks_per_sm = 0;  // 0: as many as fit
-  uint32_t spare_sms = 0;      // SMs this lane's counts leave free
   uint64_t launches = 0;
 };
 
@@ -236,7 +236,6 @@ void launcher_main(bbtc_server* s, uint32_t lane) {
     bbtc_opts o = s->opts.count;
     o.use_cuda_graph = 0;
     if (L.blocks_per_sm && (!o.blocks_per_sm || o.blocks_per_sm > L.blocks_per_sm)) o.blocks_per_sm = L.blocks_per_sm;
-    if (L.spare_sms) o.spare_sms = L.spare_sms;
     const bool fused = o.kernel == BBTC_KERNEL_FUSED || (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT);
     int rc = BBTC_OK;
     if (!fused) {
@@ -323,7 +322,6 @@ void bbtc_server_opts_default(bbtc_server_opts* o) {
   o->large_blocks_per_sm = 0;
   o->aging_ms = 50;
   o->pool_bytes = 0;
-  o->small_sms = 16;
 }
 
 int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** out) {
@@ -349,17 +347,22 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
     cudaGetLastError();
     lo = hi = 0;
   }
-  // lane 0 (small graphs) and the loaders run at the highest stream priority
+  // Stream priorities: both lanes and the small requests' loads highest, the
+  // large requests' loads lowest (lower numbers run first).
+  const int mid = hi;
   for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
     rc = bbtc_ctx_create(device, &s->lanes[l].ctx);
-    if (rc == BBTC_OK) rc = set_stream_priority(s->lanes[l].ctx, l == 0 ? hi : lo);
+    if (rc == BBTC_OK) rc = set_stream_priority(s->lanes[l].ctx, hi);
   }
   for (uint32_t i = 0; rc == BBTC_OK && i < 2 * s->opts.loaders; i++) {
     bbtc_ctx* c = nullptr;
     rc = bbtc_ctx_create(device, &c);
     if (rc == BBTC_OK) s->load_ctx.push_back(c);
-    if (rc == BBTC_OK) rc = set_stream_priority(c, i % 2 == 0 ? hi : lo);
-    if (rc == BBTC_OK && i % 2 == 1) c->layout_blocks_per_sm = 4;
+    if (rc == BBTC_OK) rc = set_stream_priority(c, i % 2 == 0 ? mid : lo);
+    if (rc == BBTC_OK && i % 2 == 1) {
+      c->layout_blocks_per_sm = 2;
+      c->upload_window = 2;
+    }
   }
   for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
     if (cudaMalloc(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess ||
@@ -379,14 +382,9 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
     return rc;
   }
   {
-    // the large lane's counts leave small_sms SMs to the small requests, and
-    // use at most 4 blocks per SM: a persistent launch ends only once its
-    // last block has been scheduled, and blocks that do not fit beside the
-    // high-priority small work at launch waited behind it for hundreds of ms
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    s->lanes[1].blocks_per_sm = s->opts.large_blocks_per_sm ? s->opts.large_blocks_per_sm : 4;
-    s->lanes[1].spare_sms = std::min<uint32_t>(s->opts.small_sms, (uint32_t)std::max(sms / 2, 1));
+    // the large lane uses at most 3 blocks per SM, so every SM keeps room
+    // for the small lane's blocks
+    s->lanes[1].blocks_per_sm = s->opts.large_blocks_per_sm ? s->opts.large_blocks_per_sm : 3;
   }
   {
     // memory freed on one stream is handed to another only once the free has

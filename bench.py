@@ -345,18 +345,25 @@ def run_serve(args):
     gaps = rng.exponential(1.0 / args.rate, size=n_req)
     arrivals = np.cumsum(gaps)
     scales = np.minimum(12 + rng.geometric(0.3, size=n_req) - 1, args.serve_max_scale)
-    picks = [pool[int(s)][int(rng.integers(len(pool[int(s)])))] for s in scales]
     pinned = []
     if args.pin:
         # request buffers in page-locked memory, as a serving front end that
-        # receives requests into pinned buffers holds them
+        # receives requests into pinned buffers holds them (copied into
+        # pinned allocations: registering numpy arrays fails for arrays that
+        # share a page with one already registered)
+        import types
         import torch
-        rt = torch.cuda.cudart()
-        for gs in pool.values():
-            for g, _ in gs:
-                for a in (g.indptr, g.indices):
-                    if a.nbytes and rt.cudaHostRegister(a.ctypes.data, a.nbytes, 0) == 0:
-                        pinned.append(a)
+
+        def pin(a):
+            t = torch.empty(max(1, a.size), dtype=torch.int32, pin_memory=True)
+            t.numpy()[:a.size] = a.view(np.int32)
+            pinned.append(t)
+            return t.numpy()[:a.size].view(np.uint32)
+
+        for s in pool:
+            pool[s] = [(types.SimpleNamespace(n=g.n, m=g.m, indptr=pin(g.indptr), indices=pin(g.indices)), c)
+                       for g, c in pool[s]]
+    picks = [pool[int(s)][int(rng.integers(len(pool[int(s)])))] for s in scales]
     srv = Server(0, loaders=args.loaders)
     # warm-up: one request per scale
     for s in sorted(pool):
@@ -407,11 +414,6 @@ def run_serve(args):
         with open(args.trace, "w") as f:
             json.dump({"fields": ["scale", "m", "submit_ns", "load_ns", "ready_ns", "launch_ns", "done_ns", "batch"],
                        "requests": trace}, f)
-    if pinned:
-        import torch
-        rt = torch.cuda.cudart()
-        for a in pinned:
-            rt.cudaHostUnregister(a.ctypes.data)
     span = (last_done - first_sub) / 1e9
     res = {"metric": METRIC, "value": edges / span, "unit": UNIT, "n_gpus": 1, "steps": n_req, "warmup": len(pool),
            "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

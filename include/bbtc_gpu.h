@@ -140,8 +140,6 @@ typedef struct bbtc_opts {
   int use_cuda_graph;        /* replay the launch sequence through a captured CUDA graph */
   int sort_tasks;            /* when tasks == NULL: 1 = cost-sorted descending (default) */
   uint32_t occupancy;        /* persistent form: register budget for 4, 6 (default) or 8 blocks per SM */
-  uint32_t spare_sms;        /* persistent form: blocks (except block 0) that start on an SM numbered below
-                                this exit at once, leaving those SMs to other streams' work (0 = none) */
 } bbtc_opts;
 
 void bbtc_opts_default(bbtc_opts* o);
@@ -245,12 +243,10 @@ typedef struct bbtc_server_opts {
   uint32_t reserved;
   bbtc_opts count;        /* launch options of every batch */
   uint64_t small_edges;   /* graphs of at most this many edges use the high-priority lane (0 = 2^22) */
-  uint32_t large_blocks_per_sm; /* persistent blocks per SM of the large lane (0 = 4) */
+  uint32_t large_blocks_per_sm; /* persistent blocks per SM of the large lane (0 = 3) */
   uint32_t aging_ms;      /* a request waiting this long is loaded before smaller ones (default 50) */
   uint64_t pool_bytes;    /* the device memory pool is grown to this size at creation, so loads never
                              wait for it to grow (0 = 1.1 x hbm_budget; at most the free memory less 8 GiB) */
-  uint32_t small_sms;     /* SMs the large lane's counts leave to small requests (spare_sms; default 16) */
-  uint32_t reserved3;
 } bbtc_server_opts;
 typedef struct bbtc_request_info {
   uint64_t count;     /* exact count once status == 1 */
