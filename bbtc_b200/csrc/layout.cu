@@ -116,30 +116,15 @@ __global__ void k_tile_base(const uint32_t* __restrict__ rp, const uint64_t* __r
     base[t] = rp[rp_off[t]];
 }
 
-// Subtract each tile's base from its slots: row pointers become tile-local.
-__global__ void k_localize(uint32_t* __restrict__ rp, uint32_t P, const uint64_t* __restrict__ part_off,
-                           const uint32_t* __restrict__ base, uint64_t len) {
-  __shared__ uint64_t poff[kMaxParts + 1];
-  for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) poff[t] = part_off[t];
-  __syncthreads();
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < len; s += stride) {
-    uint32_t lo = 0, hi = P;  // row part x: last x with part_off[x] <= s
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (poff[mid] <= s) lo = mid; else hi = mid;
-    }
-    const uint64_t A = (poff[lo + 1] - poff[lo]) / P;  // slots per tile of this row part
-    const uint32_t y = (uint32_t)((s - poff[lo]) / A);
-    rp[s] -= base[lo * P + y];
-  }
-}
-
-// Longest row and non-empty rows per tile, from the local row pointers;
-// lanes of one tile are combined before the atomics.
-__global__ void k_rowstats(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cuts_g, uint32_t P,
-                           const uint64_t* __restrict__ part_off, uint64_t len, uint32_t* __restrict__ maxdeg,
-                           uint32_t* __restrict__ nerows) {
+// One pass over the row-pointer pool: subtract each tile's base from its
+// slots (row pointers become tile-local), and per tile the longest row and
+// the number of non-empty rows.  A row's length is its run count (the scan
+// input), so the pass reads no neighbouring slot that another thread is
+// rewriting; lanes of one tile are combined before the atomics.
+__global__ void k_localize_stats(uint32_t* __restrict__ rp, const uint32_t* __restrict__ counts,
+                                 const uint32_t* __restrict__ cuts_g, uint32_t P,
+                                 const uint64_t* __restrict__ part_off, const uint32_t* __restrict__ base,
+                                 uint64_t len, uint32_t* __restrict__ maxdeg, uint32_t* __restrict__ nerows) {
   __shared__ uint32_t cuts[kMaxParts + 1];
   __shared__ uint64_t poff[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) {
@@ -155,16 +140,17 @@ __global__ void k_rowstats(const uint32_t* __restrict__ rp, const uint32_t* __re
     const uint64_t s = start + it * stride;
     uint32_t tile = 0xffffffffu, rowlen = 0;
     if (s < len) {
-      uint32_t lo = 0, hi = P;
+      uint32_t lo = 0, hi = P;  // row part x: last x with part_off[x] <= s
       while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (poff[mid] <= s) lo = mid; else hi = mid;
       }
-      const uint64_t A = (poff[lo + 1] - poff[lo]) / P;
+      const uint64_t A = (poff[lo + 1] - poff[lo]) / P;  // slots per tile of this row part
       const uint32_t y = (uint32_t)((s - poff[lo]) / A);
       const uint32_t r = (uint32_t)(s - poff[lo] - (uint64_t)y * A);
+      rp[s] -= base[lo * P + y];
       if (r < cuts[lo + 1] - cuts[lo]) {
-        rowlen = rp[s + 1] - rp[s];
+        rowlen = counts[s + 1];  // rp[s + 1] - rp[s] before or after the rebase
         tile = lo * P + y;
       }
     }
@@ -375,9 +361,8 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   uint32_t* st_nnz = d_stats;
   uint32_t* st_max = d_stats + T;
   uint32_t* st_ne = d_stats + 2 * T;
-  k_localize<<<grid, 256, 0, s>>>(bt.d_rp, P, d_part_off, base.as<uint32_t>(), part_off[P]);
-  BBTC_CUDA(cudaGetLastError());
-  k_rowstats<<<grid, 256, 0, s>>>(bt.d_rp, d_cuts, P, d_part_off, part_off[P], st_max, st_ne);
+  k_localize_stats<<<grid, 256, 0, s>>>(bt.d_rp, counts.as<uint32_t>(), d_cuts, P, d_part_off, base.as<uint32_t>(),
+                                        part_off[P], st_max, st_ne);
   BBTC_CUDA(cudaGetLastError());
   k_tile_offsets<<<1, 32, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, st_nnz, d_coloff);
   BBTC_CUDA(cudaGetLastError());

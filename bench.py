@@ -75,7 +75,7 @@ def parse():
                    help="single: one R-MAT s22 graph (default); batch: 512 R-MAT + 64 RGG graphs in one "
                         "launch; serve: Poisson request stream through the continuous-batching server")
     p.add_argument("--batch-max-scale", type=int, default=20)
-    p.add_argument("--rate", type=float, default=1000.0, help="serve: requests per second")
+    p.add_argument("--rate", type=float, default=600.0, help="serve: requests per second")
     p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     p.add_argument("--serve-max-scale", type=int, default=22)
     p.add_argument("--loaders", type=int, default=4, help="serve: loader threads")
