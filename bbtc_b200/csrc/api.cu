@@ -371,7 +371,7 @@ int bbtc_count_wait(bbtc_ctx* ctx, bbtc_graph* g, uint64_t* out) {
   BBTC_CUDA(cudaSetDevice(ctx->device));
   uint64_t* h = reinterpret_cast<uint64_t*>(ctx->h_stage + kStageOut);
   BBTC_CUDA(cudaMemcpyAsync(h, g->d_count, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  BBTC_CUDA(cudaStreamSynchronize(ctx->stream));
+  BBTC_TRY(staging_status(ctx));  // synchronises the stream
   *out = *h;
   return BBTC_OK;
 }
@@ -491,7 +491,8 @@ int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, cons
     cudaError_t e = cudaMemcpyAsync(h, d_outs, ng * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) rc = cuda_fail(e, "batch readback");
-    else if (staged) std::memcpy(outs, h, ng * sizeof(uint64_t));
+    else rc = staging_status(ctx);
+    if (rc == BBTC_OK && staged) std::memcpy(outs, h, ng * sizeof(uint64_t));
   }
   for (uint32_t i = 0; i < ng; i++) gs[i]->last_launches = plan.launches;
   plan.release();

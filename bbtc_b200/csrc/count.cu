@@ -51,7 +51,50 @@ constexpr uint32_t FULL = 0xffffffffu;
 // 8-byte aligned FusedFrame (22 words), rounded up to an even count
 constexpr uint32_t kSegWords = 96;
 constexpr uint32_t kFrameOffset = 66;  // words after the bitmap
+// per-warp bulk-staging state of the per-task kernels, after the bitmap:
+// an mbarrier (8 bytes) at kBarOffset, its phase bit and a "staging off" flag
+constexpr uint32_t kBarOffset = 92;
+constexpr uint32_t kPhaseOffset = 94;
+constexpr uint32_t kStageOffFlag = 95;
+constexpr uint32_t kStageMin = 64;         // pivot rows this long or longer are staged by one bulk copy
+constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait polls before a staging copy is given up
 constexpr uint32_t kSplitList = 128; // split pivots: room for the ids below the bitmap window
+
+// ---- bulk copies into shared memory (cp.async.bulk + mbarrier) ------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One lane: copy `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from global to shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier plain stores to dst come first
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+// Wait for the phase with parity `parity` of `bar` to complete; false when
+// it has not after kWaitLimit polls.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t x) {
   uint32_t lo = 0;
@@ -317,8 +360,94 @@ __device__ __forceinline__ uint32_t next_row(const uint32_t* __restrict__ rp, ui
 }
 
 // One per-task work unit: entries [unit*K, min((unit+1)*K, nnz)) of the rows tile.
+// Per-task pivot of the bitmap or list kind, staged in shared memory by one
+// bulk copy (cp.async.bulk, the TMA engine; completion on the warp's
+// mbarrier) of the 16-byte aligned span of the pivot row's column ids: the
+// bitmap is then set, and cleared afterwards, from shared memory, and the
+// list kind searches the staged span in place.  Returns false, having done
+// nothing, when the row is short, the span does not fit the room left in the
+// warp's buffer, or staging is off on this warp; the caller then loads the
+// row itself (pivot_pass).  The column segment of a tile starts on a 16-byte
+// boundary and the pool ends with a 16-byte tail, so the rounded span stays
+// inside the allocation.
+template <uint32_t KIND>
+__device__ __forceinline__ bool staged_pass(const uint32_t* __restrict__ tile_col, uint32_t ps, uint32_t pd,
+                                            uint32_t words, const TileSegs& segs, uint32_t e, uint32_t ee,
+                                            const uint32_t* __restrict__ prb_col, uint32_t* bm, uint32_t bm_words,
+                                            uint32_t* sstart, uint32_t* sbase, uint32_t lane, uint32_t* err,
+                                            unsigned long long& acc) {
+  uint32_t* state = bm + bm_words;
+  if (pd < kStageMin || state[kStageOffFlag]) return false;
+  const uint32_t a0 = ps & ~3u, off = ps & 3u;
+  const uint32_t span = ((ps + pd + 3u) & ~3u) - a0;  // words, a multiple of 4
+  // bitmap kind: after the bitmap and its always-zero word; list kind: the list itself
+  uint32_t* stage = KIND == kPivotList ? bm : bm + ((words + 1u + 3u) & ~3u);
+  if (span > bm_words - (uint32_t)(stage - bm)) return false;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(state + kBarOffset);
+  const uint32_t phase = state[kPhaseOffset];
+  if (lane == 0) bulk_to_shared(stage, tile_col + a0, span * 4u, bar);
+  const bool ok = bar_wait(bar, phase);
+  __syncwarp();
+  if (!ok) {
+    // the copy did not land in time: the count is void (the host sees the
+    // flag and fails the call), and this warp stages nothing more
+    if (lane == 0) {
+      atomicOr(err, 1u);
+      state[kStageOffFlag] = 1u;
+    }
+    __syncwarp();
+    return true;
+  }
+  if (lane == 0) state[kPhaseOffset] = phase ^ 1u;
+  const uint32_t* ids = stage + off;
+  if constexpr (KIND == kPivotBitmap) {
+    for (uint32_t i = lane; i < pd; i += 32) {
+      const uint32_t y = ids[i];
+      atomicOr(&bm[y >> 5], 1u << (y & 31));
+    }
+  }
+  __syncwarp();
+  PivotView pv;
+  pv.row = tile_col + ps;
+  pv.len = pd;
+  pv.base = 0;
+  pv.cap = words * 32;
+  pv.first = ids[0];
+  pv.last = ids[pd - 1];
+  pv.res = nullptr;
+  pv.rlen = 0;
+  const uint32_t hits =
+      probe_entries<KIND, false>(segs, e, ee, prb_col, KIND == kPivotList ? ids : bm, sstart, sbase, pv, lane);
+  __syncwarp();
+  // back to an all-zero buffer: the bitmap words the ids set, then the staged span
+  if constexpr (KIND == kPivotBitmap) {
+    if (pd < words) {
+      for (uint32_t i = lane; i < pd; i += 32) bm[ids[i] >> 5] = 0;
+    } else {
+      for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
+    }
+    __syncwarp();
+  }
+  for (uint32_t i = lane; i < span; i += 32) stage[i] = 0;
+  __syncwarp();
+  acc += hits;
+  return true;
+}
+
+// Set up a warp's staging state (kernel start, before any bulk copy).
+__device__ __forceinline__ void staging_init(uint32_t* bm, uint32_t bm_words, uint32_t lane) {
+  uint32_t* state = bm + bm_words;
+  if (lane == 0) {
+    bar_init(reinterpret_cast<uint64_t*>(state + kBarOffset));
+    state[kPhaseOffset] = 0;
+    state[kStageOffFlag] = 0;
+  }
+  __syncwarp();
+}
+
 __device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
-                                                     uint32_t* sstart, uint32_t* sbase, uint32_t lane) {
+                                                     uint32_t* sstart, uint32_t* sbase, uint32_t lane,
+                                                     uint32_t bm_words, uint32_t* err) {
   const uint32_t* __restrict__ r_rp = tk.rows.rp;
   const uint32_t* __restrict__ p_rp = tk.pivot.rp;
   const uint32_t* __restrict__ p_col = tk.pivot.col;
@@ -338,11 +467,15 @@ __device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t
       const uint32_t* prow = p_col + ps;
       switch (tk.kind) {
         case kPivotBitmap:
-          acc += pivot_pass<kPivotBitmap, false>(prow, pd, 0, tk.words, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase,
-                                          lane);
+          if (!staged_pass<kPivotBitmap>(p_col, ps, pd, tk.words, segs, e, ee, tk.probe.col, bm, bm_words, sstart,
+                                         sbase, lane, err, acc))
+            acc += pivot_pass<kPivotBitmap, false>(prow, pd, 0, tk.words, 0, segs, e, ee, tk.probe.col, bm, sstart,
+                                                   sbase, lane);
           break;
         case kPivotList:
-          acc += pivot_pass<kPivotList, false>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
+          if (!staged_pass<kPivotList>(p_col, ps, pd, 0, segs, e, ee, tk.probe.col, bm, bm_words, sstart, sbase, lane,
+                                       err, acc))
+            acc += pivot_pass<kPivotList, false>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
           break;
         default:
           acc += pivot_pass<kPivotGlobal, false>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
@@ -413,9 +546,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 
 __device__ __forceinline__ unsigned long long dispatch_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
                                                             uint32_t* sstart, uint32_t* sbase, uint32_t lane,
-                                                            uint32_t bm_words) {
+                                                            uint32_t bm_words, uint32_t* err) {
   if (tk.kind == kFusedRow) return fused_unit(tk, unit, bm, sstart, sbase, lane, bm_words);
-  return task_unit(tk, unit, bm, sstart, sbase, lane);
+  return task_unit(tk, unit, bm, sstart, sbase, lane, bm_words, err);
 }
 
 // Persistent form: every warp claims units from one head until the queue is
@@ -430,8 +563,9 @@ __global__ void __launch_bounds__(256, MINB) k_count_queue(const DevTask* __rest
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
   uint32_t* sstart = bm + bm_words;
   uint32_t* sbase = sstart + 33;
+  uint32_t* err = head + 1;  // set when a staging copy gave up
   for (uint32_t i = lane; i < bm_words; i += 32) bm[i] = 0;
-  __syncwarp();
+  staging_init(bm, bm_words, lane);
   while (true) {
     uint32_t g = 0;
     if (lane == 0) g = atomicAdd(head, 1u);
@@ -443,26 +577,28 @@ __global__ void __launch_bounds__(256, MINB) k_count_queue(const DevTask* __rest
       if (prefix[mid] <= g) lo = mid; else hi = mid;
     }
     const DevTask& tk = tasks[lo];
-    const unsigned long long c = warp_sum(dispatch_unit(tk, g - prefix[lo], bm, sstart, sbase, lane, bm_words));
+    const unsigned long long c =
+        warp_sum(dispatch_unit(tk, g - prefix[lo], bm, sstart, sbase, lane, bm_words, err));
     if (lane == 0 && c) atomicAdd(&outs[tk.slot], c);
   }
 }
 
 // Plain form: one task per launch; warps stride over the task's units.
 __global__ void __launch_bounds__(256, 4) k_count_task(const DevTask* __restrict__ task, uint32_t units,
-                                                       unsigned long long* __restrict__ outs, uint32_t bm_words) {
+                                                       unsigned long long* __restrict__ outs, uint32_t bm_words,
+                                                       uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) uint32_t sh[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
   uint32_t* sstart = bm + bm_words;
   uint32_t* sbase = sstart + 33;
   for (uint32_t i = lane; i < bm_words; i += 32) bm[i] = 0;
-  __syncwarp();
+  staging_init(bm, bm_words, lane);
   const DevTask& tk = *task;
   const uint32_t wpb = blockDim.x >> 5;
   unsigned long long acc = 0;
   for (uint32_t u = blockIdx.x * wpb + warp; u < units; u += gridDim.x * wpb)
-    acc += dispatch_unit(tk, u, bm, sstart, sbase, lane, bm_words);
+    acc += dispatch_unit(tk, u, bm, sstart, sbase, lane, bm_words, err);
   acc = warp_sum(acc);
   if (lane == 0 && acc) atomicAdd(&outs[tk.slot], acc);
 }
@@ -922,6 +1058,7 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
   const size_t sm = smem_bytes(bmw, wpb);
   auto* outs = reinterpret_cast<unsigned long long*>(d_outs);
   BBTC_CUDA(cudaMemsetAsync(d_outs, 0, nouts * sizeof(uint64_t), s));
+  BBTC_CUDA(cudaMemsetAsync(ctx->d_unit_counter, 0, 2 * sizeof(uint32_t), s));  // queue head, staging flag
   plan->launches = 0;
   const uint32_t ntasks = (uint32_t)plan->tasks.size();
   if (ntasks == 0) return BBTC_OK;
@@ -929,7 +1066,7 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
     for (uint32_t t = 0; t < ntasks; t++) {
       const uint32_t units = plan->prefix[t + 1] - plan->prefix[t];
       const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>((units + wpb - 1) / wpb, ctx->sms * 8));
-      k_count_task<<<grid, wpb * 32, sm, s>>>(plan->d_tasks + t, units, outs, bmw);
+      k_count_task<<<grid, wpb * 32, sm, s>>>(plan->d_tasks + t, units, outs, bmw, ctx->d_unit_counter + 1);
       BBTC_CUDA(cudaGetLastError());
       plan->launches++;
     }
@@ -946,12 +1083,19 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
     // leaves the rest of the GPU to other streams)
     const uint64_t want = ((uint64_t)plan->total_units + wpb - 1) / wpb;
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ctx->sms * per_sm, want));
-    BBTC_CUDA(cudaMemsetAsync(ctx->d_unit_counter, 0, sizeof(uint32_t), s));
     kern<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units, ctx->d_unit_counter,
                                     outs, bmw);
     BBTC_CUDA(cudaGetLastError());
     plan->launches = 1;
   }
+  return BBTC_OK;
+}
+
+int staging_status(bbtc_ctx* ctx) {
+  uint32_t* h = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageBad);
+  BBTC_CUDA(cudaMemcpyAsync(h, ctx->d_unit_counter + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BBTC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (*h) return fail(BBTC_ERR_TIMEOUT, "a shared-memory staging copy did not complete; the count is void");
   return BBTC_OK;
 }
 

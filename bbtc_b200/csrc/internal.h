@@ -197,6 +197,9 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
                   const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o, bool fused,
                   uint64_t* d_outs, Plan* plan, bool reuse);
 int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o);
+// After a count has finished on ctx's stream: BBTC_ERR_TIMEOUT if a
+// shared-memory staging copy of the launch gave up waiting (the count is void).
+int staging_status(bbtc_ctx* ctx);
 size_t smem_bytes_for(const bbtc_opts& o);
 
 }  // namespace bbtc

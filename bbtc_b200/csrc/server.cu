@@ -254,6 +254,7 @@ void launcher_main(bbtc_server* s, uint32_t lane) {
                           ctx->stream);
       const cudaError_t e2 = e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
       if (e2 != cudaSuccess) rc = cuda_fail(e2, "server batch readback");
+      else rc = staging_status(ctx);
     }
     const uint64_t t = now_ns();
     // stream-ordered frees: the memory returns to the pool behind this launch

@@ -295,3 +295,23 @@ def test_small_grids(ctx, kernel):
         want = oracle.count(g.n, g.indptr, g.indices, cuts)
         got = gpu_count(ctx, g, cuts, kernel=kernel, mode="persistent", cuda_graph=False)
         assert got == want, s
+
+
+@pytest.mark.parametrize("mode", ["persistent", "plain"])
+@pytest.mark.parametrize("kernel", ["bitmap", "search"])
+def test_bulk_staged_pivots(ctx, kernel, mode):
+    """Per-task pivot rows of 64 ids or more are staged in shared memory by a
+    bulk copy (the bitmap kind sets its bitmap from the staged ids, the list
+    kind searches them in place); a skewed graph cut in few parts has many
+    such tile rows, at every 16-byte misalignment of their start."""
+    g = graphs.rmat(16, 16, seed=1)
+    for P in (2, 4, 8):
+        cuts = graphs.cuts(g, P, "uni")
+        # the longest row of a tile, from the host CSR: staging needs >= 64 ids
+        ip, ix = g.indptr.astype(np.int64), g.indices.astype(np.int64)
+        part = np.searchsorted(cuts, ix, side="right") - 1
+        row = np.repeat(np.arange(g.n), np.diff(ip))
+        longest = np.bincount(row * P + part).max()
+        assert longest >= 64, longest
+        want = oracle.count(g.n, g.indptr, g.indices, cuts)
+        assert gpu_count(ctx, g, cuts, kernel=kernel, mode=mode, cuda_graph=False) == want, P
