@@ -311,13 +311,13 @@ void bbtc_opts_default(bbtc_opts* o) {
   std::memset(o, 0, sizeof(*o));
   o->mode = BBTC_MODE_PERSISTENT;
   o->kernel = BBTC_KERNEL_AUTO;
-  o->bitmap_words = 1024;
+  o->bitmap_words = 0;  // by graph size (count.cu: resolve_opts)
   o->warps_per_block = 8;
   o->unit_work = 0;
   o->blocks_per_sm = 0;
   o->use_cuda_graph = 1;
   o->sort_tasks = 1;
-  o->occupancy = 6;
+  o->occupancy = 0;  // by bitmap size
 }
 
 static int count_async_impl(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint32_t ntasks, int32_t border,

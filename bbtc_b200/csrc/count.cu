@@ -120,6 +120,32 @@ struct PivotView {
   uint32_t rlen;
 };
 
+// First p in [from, n) with a[p] >= x (n if none) for a sorted a, given
+// a[from - 1] < x: steps of 1, 2, 4, ... from `from`, then bisection of the
+// last step.  A lane probing increasing ids of one row against a long pivot
+// row moves forward from its previous position instead of bisecting the
+// whole row again (skewed degrees: long pivot rows, short probe rows).
+__device__ __forceinline__ uint32_t gallop_lb(const uint32_t* __restrict__ a, uint32_t n, uint32_t from, uint32_t x) {
+  if (from >= n || a[from] >= x) return from;
+  uint32_t lo = from, step = 1;  // a[lo] < x
+  while (lo + step < n && a[lo + step] < x) {
+    lo += step;
+    step <<= 1;
+  }
+  uint32_t L = lo + 1;
+  uint32_t len = min(lo + step, n) - L;  // the answer is in [L, L + len]
+  while (len > 0) {
+    const uint32_t half = len >> 1;
+    if (a[L + half] < x) {
+      L += half + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  return L;
+}
+
 template <uint32_t KIND>
 __device__ __forceinline__ uint32_t member(const uint32_t* bm, const PivotView& pv, uint32_t x) {
   if constexpr (KIND == kPivotBitmap) {
@@ -228,6 +254,7 @@ __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, 
       if (sstart[owner + step] <= lane) owner += step;
     uint32_t nb = sstart[owner + 1];
     uint32_t bs = sbase[owner];
+    uint32_t gown = 0xffffffffu, gpos = 0;  // global kind: probe row and position of the last search
     for (uint32_t c = 0; c < total; c += 128) {
       if constexpr (WORDS) {
         const uint2* __restrict__ words = reinterpret_cast<const uint2*>(prb_col);
@@ -252,6 +279,7 @@ __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, 
       } else {
         uint32_t x[4];
         bool ok[4];
+        uint32_t own[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           const uint32_t id = c + 32u * k + lane;
@@ -265,9 +293,26 @@ __device__ __forceinline__ uint32_t probe_entries(const Segs& segs, uint32_t e, 
             }
             x[k] = __ldg(prb_col + bs + id);
           }
+          own[k] = owner;
         }
+        if constexpr (KIND == kPivotGlobal) {
+          // galloping search in the pivot row from this lane's last position
+          // in the same probe row (ids of one row come in increasing order)
 #pragma unroll
-        for (int k = 0; k < 4; k++) hits += ok[k] ? member<KIND>(bm, pv, x[k]) : 0u;
+          for (int k = 0; k < 4; k++) {
+            if (!ok[k]) continue;
+            if (own[k] != gown) {
+              gown = own[k];
+              gpos = 0;
+            }
+            if (x[k] < pv.first || x[k] > pv.last) continue;
+            gpos = gallop_lb(pv.row, pv.len, gpos, x[k]);
+            hits += (gpos < pv.len && pv.row[gpos] == x[k]) ? 1u : 0u;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; k++) hits += ok[k] ? member<KIND>(bm, pv, x[k]) : 0u;
+        }
       }
     }
     __syncwarp();
@@ -1099,10 +1144,28 @@ int staging_status(bbtc_ctx* ctx) {
   return BBTC_OK;
 }
 
+// Options left at 0 ("auto") resolved for the request's graphs.  The
+// bitmap: 1024 words per warp, 2048 once a graph has 2^24 vertices or more
+// (R-MAT s22: 8.8 ms with 1024 against 10.7 with 2048; s24: 71 ms with 2048
+// against 114 with 1024 -- the wider id space puts more of each pivot row
+// outside a 1024-word window).  Occupancy: 6 blocks per SM (40 registers)
+// while the bitmap leaves shared memory for them, else 4 (64 registers).
+static bbtc_opts resolve_opts(const std::vector<bbtc_graph*>& graphs, const bbtc_opts& in) {
+  bbtc_opts o = in;
+  if (!o.bitmap_words) {
+    uint32_t n = 0;
+    for (const bbtc_graph* g : graphs) n = std::max(n, g->n);
+    o.bitmap_words = n >= (1u << 24) ? 2048 : 1024;
+  }
+  if (!o.occupancy) o.occupancy = norm_bm_words(o.bitmap_words) <= 1024 ? 6 : 4;
+  return o;
+}
+
 int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
-                  const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& o, bool fused,
+                  const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& in, bool fused,
                   uint64_t* d_outs, Plan* plan, bool reuse) {
   cudaStream_t s = ctx->stream;
+  const bbtc_opts o = resolve_opts(graphs, in);
   BBTC_TRY(kernel_smem_optin(ctx, o));
   if (!reuse) {
     if (plan->exec) cudaGraphExecDestroy(plan->exec);

@@ -133,13 +133,14 @@ typedef enum bbtc_kernel {
 typedef struct bbtc_opts {
   int mode;                  /* bbtc_mode */
   int kernel;                /* bbtc_kernel */
-  uint32_t bitmap_words;     /* shared bitmap / list words per warp: 0 = default (1024) */
+  uint32_t bitmap_words;     /* shared bitmap / list words per warp: 0 = by graph size (1024; 2048 from 2^24 vertices) */
   uint32_t warps_per_block;  /* 0 = default (8) */
   uint32_t unit_work;        /* target probes per work unit, 0 = default (256 task rows, 8192 tasks) */
   uint32_t blocks_per_sm;    /* persistent grid = SMs x this, 0 = occupancy limit */
   int use_cuda_graph;        /* replay the launch sequence through a captured CUDA graph */
   int sort_tasks;            /* when tasks == NULL: 1 = cost-sorted descending (default) */
-  uint32_t occupancy;        /* persistent form: register budget for 4, 6 (default) or 8 blocks per SM */
+  uint32_t occupancy;        /* persistent form: register budget for 4, 6 or 8 blocks per SM (0: 6 with a
+                                bitmap of at most 1024 words, else 4) */
 } bbtc_opts;
 
 void bbtc_opts_default(bbtc_opts* o);

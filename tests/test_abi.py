@@ -33,7 +33,8 @@ def test_version_and_defaults():
     assert core.lib().bbtc_version() >= 10000
     o = core.options()
     assert o.mode == core.MODE_PERSISTENT and o.kernel == core.KERNEL_AUTO
-    assert o.bitmap_words == 1024 and o.warps_per_block == 8 and o.use_cuda_graph == 1
+    assert o.bitmap_words == 0 and o.occupancy == 0  # resolved per request from the graphs' size
+    assert o.warps_per_block == 8 and o.use_cuda_graph == 1
 
 
 def test_task_list_matches_reference_enumeration():
