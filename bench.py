@@ -594,8 +594,8 @@ def main():
                    "layout_ms_first": layout_ms,
                    "layout_ms": e2e["layout_ms"] if e2e else layout_ms, "device_bytes": device_bytes, "generate_s": round(gen_s, 2),
                    "l2": "block CSR larger than L2, plus a 256 MiB fill between timed steps (excluded)",
-                   "launch": {f: getattr(o, f) for f in ("bitmap_words", "warps_per_block", "unit_work",
-                                                         "occupancy")}, "autotuned": tuned is not None,
+                   "launch": {f: (getattr(o, f) or "auto") for f in ("bitmap_words", "warps_per_block", "unit_work",
+                                                                       "occupancy")}, "autotuned": tuned is not None,
                    "parallelism": "replicas per GPU" if world > 1 else "single GPU"},
         "plain": plain,
         "e2e": e2e,
