@@ -10,7 +10,7 @@
 //     lowest priority, layout grids capped at 2 blocks per SM, at most two
 //     8 MiB upload pieces queued at a time), and queue it on its size
 //     class's lane.  A request that could never fit fails with
-//     BBTC_ERR_CAPACITY.  With two or more loaders the first one takes small
+//     BBTC_ERR_CAPACITY.  With two or more loaders half of them take small
 //     requests only.
 //   two launcher threads (lanes), each with its own highest-priority stream:
 //     lane 0 counts graphs of at most small_edges edges, lane 1 the larger
@@ -421,9 +421,10 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
       cudaGetLastError();  // not fatal: the pool grows on demand instead
     }
   }
-  // with two or more loaders, the first takes small requests only
+  // with two or more loaders, half of them (rounded down) take small requests only
+  const uint32_t small_only = s->opts.loaders > 1 ? s->opts.loaders / 2 : 0;
   for (size_t i = 0; i < s->opts.loaders; i++)
-    s->loaders.emplace_back(loader_main, s, s->load_ctx[2 * i], s->load_ctx[2 * i + 1], i == 0 && s->opts.loaders > 1);
+    s->loaders.emplace_back(loader_main, s, s->load_ctx[2 * i], s->load_ctx[2 * i + 1], i < small_only);
   for (uint32_t l = 0; l < 2; l++) s->lanes[l].th = std::thread(launcher_main, s, l);
   *out = s;
   return BBTC_OK;
