@@ -116,6 +116,23 @@ __global__ void k_tile_base(const uint32_t* __restrict__ rp, const uint64_t* __r
     base[t] = rp[rp_off[t]];
 }
 
+// Zero fill of the large layout buffers on the SMs (a grid-stride kernel at
+// the stream's priority), leaving the copy engines to the uploads.
+__global__ void k_zero(uint32_t* __restrict__ p, uint64_t nwords) {
+  uint4* __restrict__ q = reinterpret_cast<uint4*>(p);
+  const uint64_t n4 = nwords / 4;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t i = t0; i < n4; i += stride) q[i] = make_uint4(0, 0, 0, 0);
+  for (uint64_t i = n4 * 4 + t0; i < nwords; i += stride) p[i] = 0;
+}
+
+int zero_fill(void* p, uint64_t bytes, cudaStream_t s, int grid) {
+  k_zero<<<grid, 256, 0, s>>>(static_cast<uint32_t*>(p), bytes / 4);  // callers pass multiples of 4 bytes
+  BBTC_CUDA(cudaGetLastError());
+  return BBTC_OK;
+}
+
 // One pass over the row-pointer pool: subtract each tile's base from its
 // slots (row pointers become tile-local), and per tile the longest row and
 // the number of non-empty rows.  A row's length is its run count (the scan
@@ -344,8 +361,8 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
     std::memcpy(h + T, part_off.data(), (P + 1) * sizeof(uint64_t));
     BBTC_CUDA(cudaMemcpyAsync(d_rp_off, h, (T + P + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
   }
-  BBTC_CUDA(cudaMemsetAsync(counts.p, 0, bt.rp_len * sizeof(uint32_t), s));
-  BBTC_CUDA(cudaMemsetAsync(bt.d_col, 0, bt.col_len * sizeof(uint32_t), s));
+  BBTC_TRY(zero_fill(counts.p, bt.rp_len * sizeof(uint32_t), s, grid));
+  BBTC_TRY(zero_fill(bt.d_col, bt.col_len * sizeof(uint32_t), s, grid));
   BBTC_CUDA(cudaMemsetAsync(d_stats, 0, 4 * T * sizeof(uint32_t), s));
   if (m > 0) {
     k_entry_count<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, counts.as<uint32_t>());
@@ -564,7 +581,7 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
       cudaGetLastError();
       return fail(BBTC_ERR_NOMEM, "device allocation of the word-compressed rows failed");
     }
-    BBTC_CUDA(cudaMemsetAsync(g->d_words, 0, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s));
+    BBTC_TRY(zero_fill(g->d_words, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s, grid));
     if (m > 0) {
       k_word_flags<<<grid, 256, 0, s>>>(d_indptr, d_indices, rows.as<uint32_t>(), m, wflags.as<uint32_t>());
       BBTC_CUDA(cudaGetLastError());
