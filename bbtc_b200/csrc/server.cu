@@ -39,6 +39,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "admission.hpp"
 #include "internal.h"
 
 namespace bbtc {
@@ -90,10 +91,9 @@ namespace bbtc {
 namespace {
 
 // One launch lane: a launcher thread with its own stream, result slots and
-// ready queue.  Lane 0 counts the small graphs on a high-priority stream;
-// lane 1 the large ones, its persistent blocks leaving the lowest-numbered
-// SMs free, so that lane 0's launches (and the loaders' layout kernels)
-// always find SMs no large count holds.
+// ready queue.  Lane 0 counts the small graphs, lane 1 the large ones with
+// its persistent grid capped per SM, so that lane 0's launches (and the
+// loaders' layout kernels) always find room on every SM.
 struct Lane {
   bbtc_ctx* ctx = nullptr;
   std::deque<Request*> ready;
@@ -133,26 +133,11 @@ constexpr size_t kPickScan = 4096;  // pending requests a loader looks at per pi
 
 uint32_t lane_of(const bbtc_server* s, const Request* r) { return r->m <= s->opts.small_edges ? 0u : 1u; }
 
-// The next request a loader takes, removed from `pending`, or nullptr.  Among
-// the requests the HBM budget admits (or that can never fit, and fail at
-// once): the oldest one that has waited `aging_ms` or more, else the one
-// with the fewest edges -- small requests overtake large loads, and large
-// ones are not starved.  A loader reserved for small requests sees only those.
+// The next request a loader takes (admission.hpp), removed from `pending`, or nullptr.
 Request* pick(bbtc_server* s, bool small_only) {
-  const uint64_t now = now_ns();
-  const uint64_t aging = (uint64_t)s->opts.aging_ms * 1000000ull;
-  size_t best = SIZE_MAX, i = 0;
-  for (auto it = s->pending.begin(); it != s->pending.end() && i < kPickScan; ++it, ++i) {
-    const Request* r = *it;
-    if (small_only && lane_of(s, r) != 0) continue;
-    const bool never = r->reserved > s->opts.hbm_budget;
-    if (!never && s->in_use + r->reserved > s->opts.hbm_budget && s->in_use != 0) continue;
-    if (now - r->t_submit >= aging) {
-      best = i;
-      break;
-    }
-    if (best == SIZE_MAX || r->m < s->pending[best]->m) best = i;
-  }
+  const AdmitLimits lim{s->opts.hbm_budget, s->in_use, s->opts.small_edges,
+                        (uint64_t)s->opts.aging_ms * 1000000ull, now_ns(), small_only, kPickScan};
+  const size_t best = admit_pick(s->pending, lim);
   if (best == SIZE_MAX) return nullptr;
   Request* r = s->pending[best];
   s->pending.erase(s->pending.begin() + (std::ptrdiff_t)best);
