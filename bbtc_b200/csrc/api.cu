@@ -320,6 +320,23 @@ void bbtc_opts_default(bbtc_opts* o) {
   o->occupancy = 0;  // by bitmap size
 }
 
+// Is `tasks` the whole task list of P parts, in any order: every (i <= j <= k)
+// exactly once, as (ab, bc, ac) = ((i,j), (j,k), (i,k))?
+static bool is_full_task_list(uint32_t P, const bbtc_task* tasks, uint32_t ntasks) {
+  if (ntasks != P * (P + 1) * (P + 2) / 6) return false;
+  std::vector<uint8_t> seen((size_t)P * P * P, 0);
+  for (uint32_t q = 0; q < ntasks; q++) {
+    const bbtc_task& t = tasks[q];
+    if (t.ab >= P * P || t.bc >= P * P) return false;
+    const uint32_t i = t.ab / P, j = t.ab % P, k = t.bc % P;
+    if (t.bc / P != j || t.ac != i * P + k || i > j || j > k) return false;
+    uint8_t& s = seen[((size_t)i * P + j) * P + k];
+    if (s) return false;
+    s = 1;
+  }
+  return true;
+}
+
 static int count_async_impl(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint32_t ntasks, int32_t border,
                             const bbtc_opts* opts) {
   if (!ctx || !g) return fail(BBTC_ERR_ARG, "NULL argument");
@@ -329,10 +346,15 @@ static int count_async_impl(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks
   if (opts) o = *opts; else bbtc_opts_default(&o);
   if (o.mode != BBTC_MODE_PLAIN && o.mode != BBTC_MODE_PERSISTENT) return fail(BBTC_ERR_ARG, "unknown mode");
   if (o.kernel < BBTC_KERNEL_AUTO || o.kernel > BBTC_KERNEL_FUSED) return fail(BBTC_ERR_ARG, "unknown kernel");
-  if (o.kernel == BBTC_KERNEL_FUSED && tasks)
-    return fail(BBTC_ERR_ARG, "fused task rows run the whole task list: pass tasks = NULL");
-  const bool fused = !tasks && (o.kernel == BBTC_KERNEL_FUSED ||
-                                (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT));
+  // The fused task rows count the whole task list at once.  A caller that
+  // passes the whole list (the reference's driver does, in its cost order)
+  // gets them too: the sum does not depend on the order, and with one device
+  // queue the border only orders the queue.
+  const bool whole = !tasks || is_full_task_list(g->P, tasks, ntasks);
+  if (o.kernel == BBTC_KERNEL_FUSED && !whole)
+    return fail(BBTC_ERR_ARG, "fused task rows run the whole task list: pass tasks = NULL or every task once");
+  const bool fused = whole && (o.kernel == BBTC_KERNEL_FUSED ||
+                               (o.kernel == BBTC_KERNEL_AUTO && o.mode == BBTC_MODE_PERSISTENT));
   BBTC_CUDA(cudaSetDevice(ctx->device));
   if (!fused) BBTC_TRY(ensure_fwd(g));  // task-list counting reads the forward block CSR
   std::vector<std::vector<bbtc_task>> tl(1);

@@ -120,14 +120,15 @@ typedef enum bbtc_mode {
 } bbtc_mode;
 
 typedef enum bbtc_kernel {
-  BBTC_KERNEL_AUTO = 0,   /* persistent form over the whole task list: fused task rows; otherwise
+  BBTC_KERNEL_AUTO = 0,   /* persistent form over the whole task list (tasks == NULL, or every task
+                             once in any order, as the reference's driver passes it): fused task rows; otherwise
                              per task: bitmap when the part fits the shared bitmap, else search */
   BBTC_KERNEL_BITMAP = 1, /* per task: pivot row of bc as a shared-memory bitmap, probes from ac */
   BBTC_KERNEL_SEARCH = 2, /* per task: pivot row of bc as a sorted shared-memory list, bisection probes */
   BBTC_KERNEL_MERGE = 3,  /* per task, the reference's row order: pivot = ac row of each ab row,
                              the bc rows it meets are searched against it */
   BBTC_KERNEL_FUSED = 4   /* task rows: the tasks (i, j, k >= j) sharing tile ab = (i, j) in one
-                             pass (needs the whole task list, tasks == NULL) */
+                             pass (needs the whole task list: tasks == NULL, or every task once) */
 } bbtc_kernel;
 
 typedef struct bbtc_opts {

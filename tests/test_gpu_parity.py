@@ -96,8 +96,14 @@ def test_per_task_counts(ctx):
             one = np.array([t], dtype=t.dtype)
             for kernel in ("auto", "merge"):
                 assert st.count(one, opts=options(kernel=kernel)) == want, (t, kernel)
-        with pytest.raises(BBTcError):  # fused task rows need the whole task list
-            st.count(st.task_list(), opts=options(kernel="fused"))
+        # the whole task list, in any order, runs as fused task rows
+        total = oracle.count(g.n, g.indptr, g.indices, cuts)
+        whole = st.task_list()
+        for kernel in ("fused", "auto"):
+            assert st.count(whole, opts=options(kernel=kernel)) == total, kernel
+            assert st.count(whole[::-1].copy(), opts=options(kernel=kernel)) == total, kernel
+        with pytest.raises(BBTcError):  # part of the list: fused task rows cannot run it
+            st.count(whole[: len(whole) // 2].copy(), opts=options(kernel="fused"))
     finally:
         st.free()
 
