@@ -243,7 +243,8 @@ def run_reference(args, rank: int):
     sample = (f"full workload per step: NoOfTriangles() over all {args.ncut * (args.ncut + 1) * (args.ncut + 2) // 6}"
               f" tasks, median of {len(timed)} steps after {args.warmup} warm-up")
     return {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "device": "host cores (rank 0 only)", "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": f"{workload_name(args)} {args.partitioner} "
