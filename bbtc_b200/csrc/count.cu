@@ -1148,16 +1148,18 @@ int staging_status(bbtc_ctx* ctx) {
 // bitmap: 1024 words per warp, 2048 once a graph has 2^24 vertices or more
 // (R-MAT s22: 8.8 ms with 1024 against 10.7 with 2048; s24: 71 ms with 2048
 // against 114 with 1024 -- the wider id space puts more of each pivot row
-// outside a 1024-word window).  Occupancy: 6 blocks per SM (40 registers)
-// while the bitmap leaves shared memory for them, else 4 (64 registers).
-static bbtc_opts resolve_opts(const std::vector<bbtc_graph*>& graphs, const bbtc_opts& in) {
+// outside a 1024-word window).  Occupancy: fused task rows 6 blocks per SM
+// (40 registers) while the bitmap leaves shared memory for them, else 4 (64
+// registers); per-task kernels 4 (R-MAT s20: bitmap 10.4 ms at 4 against
+// 12.4 at 6, search 14.4 / 15.7, merge 27.5 / 31.5).
+static bbtc_opts resolve_opts(const std::vector<bbtc_graph*>& graphs, const bbtc_opts& in, bool fused) {
   bbtc_opts o = in;
   if (!o.bitmap_words) {
     uint32_t n = 0;
     for (const bbtc_graph* g : graphs) n = std::max(n, g->n);
     o.bitmap_words = n >= (1u << 24) ? 2048 : 1024;
   }
-  if (!o.occupancy) o.occupancy = norm_bm_words(o.bitmap_words) <= 1024 ? 6 : 4;
+  if (!o.occupancy) o.occupancy = fused && norm_bm_words(o.bitmap_words) <= 1024 ? 6 : 4;
   return o;
 }
 
@@ -1165,7 +1167,7 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
                   const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& in, bool fused,
                   uint64_t* d_outs, Plan* plan, bool reuse) {
   cudaStream_t s = ctx->stream;
-  const bbtc_opts o = resolve_opts(graphs, in);
+  const bbtc_opts o = resolve_opts(graphs, in, fused);
   BBTC_TRY(kernel_smem_optin(ctx, o));
   if (!reuse) {
     if (plan->exec) cudaGraphExecDestroy(plan->exec);

@@ -140,8 +140,8 @@ typedef struct bbtc_opts {
   uint32_t blocks_per_sm;    /* persistent grid = SMs x this, 0 = occupancy limit */
   int use_cuda_graph;        /* replay the launch sequence through a captured CUDA graph */
   int sort_tasks;            /* when tasks == NULL: 1 = cost-sorted descending (default) */
-  uint32_t occupancy;        /* persistent form: register budget for 4, 6 or 8 blocks per SM (0: 6 with a
-                                bitmap of at most 1024 words, else 4) */
+  uint32_t occupancy;        /* persistent form: register budget for 4, 6 or 8 blocks per SM (0: 6 for
+                                fused task rows with a bitmap of at most 1024 words, else 4) */
 } bbtc_opts;
 
 void bbtc_opts_default(bbtc_opts* o);
