@@ -49,6 +49,20 @@ bool read_file(const char* path, std::string& buf) {
   return got == (size_t)sz;
 }
 
+// A cached CSR is trusted by nothing downstream (the host partitioners index
+// arrays with it), so it must meet the upload contract: indptr starts at 0,
+// never decreases and ends at m; every row is strictly increasing with ids < n.
+bool csr_ok(uint64_t n, uint64_t m, const uint32_t* indptr, const uint32_t* indices) {
+  if (indptr[0] != 0 || indptr[n] != m) return false;
+  for (uint64_t u = 0; u < n; u++) {
+    const uint32_t a = indptr[u], b = indptr[u + 1];
+    if (b < a) return false;
+    for (uint32_t e = a; e < b; e++)
+      if (indices[e] >= n || (e > a && indices[e - 1] >= indices[e])) return false;
+  }
+  return true;
+}
+
 bool ends_with(const std::string& s, const std::string& t) {
   return s.size() >= t.size() && s.compare(s.size() - t.size(), t.size(), t) == 0;
 }
@@ -121,10 +135,14 @@ int bbtcio_read(const char* path, int* kind, void** handle) {
     std::memcpy(hdr, b.data() + off, sizeof(hdr));
     off += sizeof(hdr);
     const uint64_t n = hdr[0], m = hdr[1];
-    if (b.size() < off + 4 * (n + 1) + 4 * m) return -1;
-    const uint32_t* indptr = reinterpret_cast<const uint32_t*>(b.data() + off);
-    const uint32_t* indices = reinterpret_cast<const uint32_t*>(b.data() + off + 4 * (n + 1));
-    return bbtcg_from_csr((uint32_t)n, indptr, indices, m, handle);
+    if (b.size() < off + 4 * (n + 1) + 4 * m) return -1;  // truncated
+    if (n >= 0xffffffffull) return -3;
+    // the arrays start 30 bytes in: copy them out to aligned storage
+    std::vector<uint32_t> indptr((size_t)n + 1), indices((size_t)m);
+    std::memcpy(indptr.data(), b.data() + off, 4 * (n + 1));
+    if (m) std::memcpy(indices.data(), b.data() + off + 4 * (n + 1), 4 * m);
+    if (!csr_ok(n, m, indptr.data(), indices.data())) return -1;
+    return bbtcg_from_csr((uint32_t)n, indptr.data(), indices.data(), m, handle);
   }
   std::vector<uint32_t> src, dst;
   uint64_t maxid = 0;
