@@ -23,7 +23,8 @@ from . import _lib
 c = ctypes
 
 STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_INPUT", -5: "ERR_TIMEOUT",
-          -6: "ERR_NODEV", -7: "ERR_UNSUPPORTED", -8: "ERR_STATE", -9: "ERR_CAPACITY"}
+          -6: "ERR_NODEV", -7: "ERR_UNSUPPORTED", -8: "ERR_STATE", -9: "ERR_CAPACITY",
+          -10: "ERR_LAYOUT"}
 
 MODE_PERSISTENT, MODE_PLAIN = 0, 1
 KERNEL_AUTO, KERNEL_BITMAP, KERNEL_SEARCH, KERNEL_MERGE, KERNEL_FUSED = 0, 1, 2, 3, 4
@@ -77,6 +78,7 @@ def lib() -> ctypes.CDLL:
         "bbtc_graph_free": [vp],
         "bbtc_graph_info_get": [vp, c.POINTER(GraphInfo)],
         "bbtc_graph_tile_stats": [vp, vp, vp, vp, vp, vp],
+        "bbtc_graph_validate": [vp],
         "bbtc_task_list": [u32, vp, u32, c.POINTER(u32)],
         "bbtc_sort_tasks": [vp, vp, u32, c.c_int],
         "bbtc_count": [vp, vp, vp, u32, i32, c.POINTER(Opts), c.POINTER(u64)],
@@ -239,6 +241,10 @@ class Graph:
         check(lib().bbtc_graph_tile_stats(self.handle, nnz.ctypes.data, h.ctypes.data, w.ctypes.data,
                                           deg.ctypes.data, mx.ctypes.data))
         return dict(nnz=nnz, height=h, width=w, tile_deg=deg, max_deg=mx)
+
+    def validate(self) -> None:
+        """Copy the device layout back and check it on the host (BBTcError -10 if broken)."""
+        check(lib().bbtc_graph_validate(self.handle))
 
     def task_list(self, sorted: bool = True, descending: bool = True) -> np.ndarray:
         t = task_list(self.P)

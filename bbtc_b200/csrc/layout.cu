@@ -31,6 +31,7 @@
 #include <cstring>
 
 #include "internal.h"
+#include "layout_check.hpp"
 
 namespace bbtc {
 
@@ -680,3 +681,65 @@ int ensure_fwd(bbtc_graph* g) {
 }
 
 }  // namespace bbtc
+
+// Read the whole layout back and check it on the host (debug aid: it copies
+// every array, so it costs about the graph's device bytes in host memory and
+// PCIe time).  The forward block CSR is checked when it has been built.
+int bbtc_graph_validate(const bbtc_graph* g) {
+  using namespace bbtc;
+  static_assert(check::kNoSeg == kNoSegment, "empty-tile marker");
+  if (!g) return fail(BBTC_ERR_ARG, "NULL graph");
+  bbtc_ctx* ctx = g->ctx;
+  cudaStream_t s = ctx->stream;
+  BBTC_CUDA(cudaSetDevice(ctx->device));
+  const uint32_t n = g->n;
+  const uint64_t m = g->m;
+  const uint64_t mm = std::max<uint64_t>(m, 1);
+  auto get = [&](std::vector<uint32_t>& h, const void* d, uint64_t words) -> int {
+    h.assign(words, 0);
+    if (words) BBTC_CUDA(cudaMemcpyAsync(h.data(), d, words * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    return BBTC_OK;
+  };
+  std::vector<uint32_t> indptr, indices, wptr, pairs;
+  BBTC_TRY(get(indptr, g->d_indptr, (uint64_t)n + 1));
+  BBTC_TRY(get(indices, g->d_indices, mm));
+  BBTC_TRY(get(wptr, g->d_wptr, (uint64_t)n + 1));
+  BBTC_TRY(get(pairs, g->d_words, 2 * mm));
+  BBTC_CUDA(cudaStreamSynchronize(s));
+  check::Csr c{n, m, indptr.data(), indices.data()};
+  check::Words w{wptr.data(), pairs.data(), mm};
+  std::string why = check::csr(c);
+  if (why.empty()) why = check::words(c, w);
+  std::vector<uint32_t> tp, tc;
+  if (why.empty()) check::transpose(c, tp, tc);
+  const check::Csr tr{n, m, tp.data(), tc.data()};
+  for (int pass = 0; pass < 2 && why.empty(); pass++) {
+    const BlockTiles& bt = pass == 0 ? g->rev : g->fwd;
+    if (pass == 1 && !g->fwd_built) break;
+    std::vector<uint32_t> rp, col, erow, rec;
+    BBTC_TRY(get(rp, bt.d_rp, bt.rp_len));
+    BBTC_TRY(get(col, bt.d_col, bt.col_len));
+    BBTC_TRY(get(erow, bt.d_erow, bt.erow_len));
+    if (bt.d_rec) BBTC_TRY(get(rec, bt.d_rec, 2 * bt.col_len));
+    BBTC_CUDA(cudaStreamSynchronize(s));
+    check::Tiles t;
+    t.P = g->P;
+    t.cuts = g->cuts.data();
+    t.rp_off = bt.rp_off.data();
+    t.col_off = bt.col_off.data();
+    t.nnz = bt.nnz.data();
+    t.maxdeg = bt.maxdeg.data();
+    t.nerows = bt.nerows.data();
+    t.rp = rp.data();
+    t.rp_len = bt.rp_len;
+    t.col = col.data();
+    t.col_len = bt.col_len;
+    t.erow = erow.data();
+    t.erow_len = bt.erow_len;
+    t.rec = bt.d_rec ? rec.data() : nullptr;
+    if (pass == 0 && !t.rec) why = "reversed tiles: no forward-edge records";
+    else why = check::tiles(pass == 0 ? "reversed tiles" : "forward tiles", pass == 0 ? tr : c, t, w);
+  }
+  if (!why.empty()) return fail(BBTC_ERR_LAYOUT, "device layout check failed: " + why);
+  return BBTC_OK;
+}

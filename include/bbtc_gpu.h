@@ -37,7 +37,8 @@ typedef enum bbtc_status {
   BBTC_ERR_NODEV = -6,       /* no usable CUDA device / wrong device index */
   BBTC_ERR_UNSUPPORTED = -7, /* valid request this build does not serve */
   BBTC_ERR_STATE = -8,       /* call out of order (e.g. polling an unknown request) */
-  BBTC_ERR_CAPACITY = -9     /* admission refused: over the HBM budget or slot limit */
+  BBTC_ERR_CAPACITY = -9,    /* admission refused: over the HBM budget or slot limit */
+  BBTC_ERR_LAYOUT = -10      /* bbtc_graph_validate found the device layout broken */
 } bbtc_status;
 
 typedef struct bbtc_ctx bbtc_ctx;
@@ -90,6 +91,18 @@ typedef struct bbtc_graph_info {
   double layout_ms;       /* device time of the layout build */
 } bbtc_graph_info;
 int bbtc_graph_info_get(const bbtc_graph* g, bbtc_graph_info* info);
+
+/* Debug check of the device layout: copies every array of g back and checks
+ * on the host what the counting kernels rely on -- the CSR contract; the
+ * word-compressed rows expand to the rows; every tile's row pointers start
+ * at 0, never decrease and end at its nnz; segments start on 16-byte
+ * boundaries, stay inside their pools and do not overlap; tile rows are
+ * strictly increasing, columns < the tile width, and together hold every
+ * edge exactly once; tile statistics, the row index of every 32nd entry and
+ * the reversed tiles' forward-edge records are right.  BBTC_ERR_LAYOUT with
+ * the first broken rule in the message.  Costs about the graph's device
+ * bytes in host memory; synchronises the context's stream. */
+int bbtc_graph_validate(const bbtc_graph* g);
 
 /* Per-tile statistics, row-major over the P x P grid (any pointer may be
  * NULL).  nnz / height are the reference's GetNNZ / GetHeight

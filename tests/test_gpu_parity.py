@@ -273,6 +273,32 @@ def test_tile_stats_match_reference_layout(ctx):
         st.free()
 
 
+def test_device_layout_validates(ctx):
+    """The device-built layout read back and checked on the host: reversed
+    tiles and word rows after upload, forward tiles once built, over several
+    families, partitioners, empty parts, phantom rows, P = 1 and P = 64."""
+    cases = []
+    g = graphs.rmat(12, 16, seed=7)
+    cases += [(g, graphs.cuts(g, 8, "pal")), (g, graphs.cuts(g, 5, "n1d")), (g, graphs.cuts(g, 1, "uni")),
+              (g, np.array([0, 0, 900, 900, 2500, g.n + 3], np.uint32)),
+              (g, np.array(list(range(0, 64 * 64, 64)) + [g.n], np.uint32))]
+    cl = graphs.chung_lu(20000, seed=3)
+    cases.append((cl, graphs.cuts(cl, 16, "n1d")))
+    rg = graphs.rgg(1 << 14, seed=100)
+    cases.append((rg, graphs.cuts(rg, 6, "uni")))
+    empty = graphs.from_pairs(10, [], [])
+    cases.append((empty, graphs.cuts(empty, 3, "uni")))
+    for g, cuts in cases:
+        st = Graph.from_csr(ctx, g, cuts)
+        try:
+            st.validate()
+            st.tile_stats()  # builds the forward block CSR
+            st.validate()
+            assert st.count() == oracle.count(g.n, g.indptr, g.indices, cuts)
+        finally:
+            st.free()
+
+
 @pytest.mark.parametrize("bitmap_words", [16, 64, 256])
 def test_mixed_pivot_kinds_in_one_queue(ctx, bitmap_words):
     """pal cuts give parts of very different widths, so one persistent launch
