@@ -69,6 +69,7 @@ def lib() -> ctypes.CDLL:
     sig = {
         "bbtc_last_error": [c.c_char_p, c.c_size_t],
         "bbtc_version": [],
+        "bbtc_debug_fail_alloc": [c.c_int64, c.POINTER(c.c_int64)],
         "bbtc_ctx_create": [c.c_int, c.POINTER(vp)],
         "bbtc_ctx_destroy": [vp],
         "bbtc_ctx_stream": [vp, c.POINTER(vp)],
@@ -101,6 +102,16 @@ def last_error() -> str:
     buf = c.create_string_buffer(1024)
     lib().bbtc_last_error(buf, len(buf))
     return buf.value.decode(errors="replace")
+
+
+def debug_fail_alloc(after: int) -> int:
+    """Test hook: fail the device allocation that follows `after` more
+    successful ones (after < 0 disarms).  Returns the previous state: -1 when
+    nothing was armed or the armed fault has fired, else the allocations it
+    was still to let pass."""
+    left = c.c_int64()
+    check(lib().bbtc_debug_fail_alloc(int(after), c.byref(left)))
+    return left.value
 
 
 def check(rc: int) -> None:

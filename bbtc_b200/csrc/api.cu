@@ -1,7 +1,9 @@
 // C ABI of libbbtc.so: contexts, graphs, task lists and counting.
 // The mapping to the reference's classes is given in include/bbtc_gpu.h.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -18,6 +20,20 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 int fail(int status, const std::string& msg) {
   set_error(msg);
   return status;
+}
+
+// Armed allocation fault: k >= 0 lets k more device allocations pass and fails
+// the next one; -1 is disarmed.
+static std::atomic<int64_t> g_alloc_fault{[] {
+  const char* v = std::getenv("BBTC_FAIL_ALLOC");
+  return v && *v ? (int64_t)std::strtoll(v, nullptr, 10) : (int64_t)-1;
+}()};
+
+bool take_alloc_fault() {
+  int64_t v = g_alloc_fault.load(std::memory_order_relaxed);
+  while (v >= 0)
+    if (g_alloc_fault.compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) return v == 0;
+  return false;
 }
 
 int cuda_fail(cudaError_t e, const char* what) {
@@ -79,7 +95,7 @@ int finish_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* indptr, const uint3
   g->m = m;
   g->P = P;
   g->cuts.assign(cuts, cuts + P + 1);
-  if (cudaMallocAsync(&g->d_count, 64 * sizeof(uint64_t), ctx->stream) != cudaSuccess) {
+  if (dev_malloc(&g->d_count, 64 * sizeof(uint64_t), ctx->stream) != cudaSuccess) {
     cudaGetLastError();
     delete g;
     return fail(BBTC_ERR_NOMEM, "device allocation of the result slot failed");
@@ -124,6 +140,12 @@ int bbtc_last_error(char* buf, size_t len) {
 
 int bbtc_version(void) { return 10000; }
 
+int bbtc_debug_fail_alloc(int64_t after, int64_t* left) {
+  const int64_t prev = g_alloc_fault.exchange(after < 0 ? -1 : after);
+  if (left) *left = prev < 0 ? -1 : prev;
+  return BBTC_OK;
+}
+
 int bbtc_ctx_create(int device, bbtc_ctx** out) {
   if (!out) return fail(BBTC_ERR_ARG, "out is NULL");
   *out = nullptr;
@@ -158,7 +180,7 @@ int bbtc_ctx_create(int device, bbtc_ctx** out) {
     }
     cudaGetLastError();
   }
-  e = cudaMalloc(&c->d_unit_counter, 64 * sizeof(uint32_t));
+  e = dev_malloc_sync(&c->d_unit_counter, 64 * sizeof(uint32_t));
   if (e != cudaSuccess) {
     cudaStreamDestroy(c->stream);
     delete c;
@@ -496,7 +518,7 @@ int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, cons
     tl[i] = default_tasks(gs[i], !fused_all && o.sort_tasks != 0);
   }
   uint64_t* d_outs = nullptr;
-  BBTC_CUDA(cudaMallocAsync(&d_outs, ng * sizeof(uint64_t), ctx->stream));
+  BBTC_CUDA(dev_malloc(&d_outs, ng * sizeof(uint64_t), ctx->stream));
   struct F {
     uint64_t* p;
     cudaStream_t s;

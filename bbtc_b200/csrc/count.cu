@@ -1179,8 +1179,8 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
         plan->release();
         plan->stream = s;
         const size_t cap = std::max<size_t>(nt, 256);
-        if (cudaMallocAsync(&plan->d_tasks, cap * sizeof(DevTask), s) != cudaSuccess ||
-            cudaMallocAsync(&plan->d_prefix, (cap + 1) * sizeof(uint32_t), s) != cudaSuccess) {
+        if (dev_malloc(&plan->d_tasks, cap * sizeof(DevTask), s) != cudaSuccess ||
+            dev_malloc(&plan->d_prefix, (cap + 1) * sizeof(uint32_t), s) != cudaSuccess) {
           cudaGetLastError();
           plan->release();
           return fail(BBTC_ERR_NOMEM, "device allocation of the task queue failed");

@@ -30,6 +30,33 @@ int cuda_fail(cudaError_t e, const char* what);
     if (rc__ != BBTC_OK) return rc__; \
   } while (0)
 
+// ---- device allocations ---------------------------------------------------
+// Every device allocation of the library whose failure is an error goes
+// through dev_malloc / dev_malloc_sync, so that a test hook
+// (bbtc_debug_fail_alloc, or BBTC_FAIL_ALLOC=k in the environment when the
+// library loads) can make the k-th next one fail as if the device were out of
+// memory.  take_alloc_fault() consumes the armed fault (true once, when the
+// count reaches it).
+bool take_alloc_fault();
+
+template <class T>
+inline cudaError_t dev_malloc(T** p, size_t bytes, cudaStream_t s) {
+  if (take_alloc_fault()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocAsync(reinterpret_cast<void**>(p), bytes, s);
+}
+
+template <class T>
+inline cudaError_t dev_malloc_sync(T** p, size_t bytes) {
+  if (take_alloc_fault()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
 constexpr uint32_t kMaxParts = 64;
 constexpr uint32_t kMaxDevices = 64;
 constexpr uint64_t kNoSegment = ~0ull;
@@ -144,7 +171,7 @@ struct DevBuf {
 
 inline int dalloc(DevBuf& b, size_t bytes, cudaStream_t s) {
   b.s = s;
-  cudaError_t e = cudaMallocAsync(&b.p, bytes > 16 ? bytes : 16, s);
+  cudaError_t e = dev_malloc(&b.p, bytes > 16 ? bytes : 16, s);
   if (e != cudaSuccess) {
     cudaGetLastError();
     b.p = nullptr;

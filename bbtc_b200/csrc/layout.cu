@@ -338,10 +338,10 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   bt.col_len = m + 4ull * T + 4;
   bt.erow_len = bt.col_len / 32 + T + 1;  // tile t's index starts at col_off[t] / 32 + t
   {
-    cudaError_t e1 = cudaMallocAsync(&bt.d_rp, bt.rp_len * sizeof(uint32_t), s);
-    cudaError_t e2 = cudaMallocAsync(&bt.d_col, bt.col_len * sizeof(uint32_t), s);
-    cudaError_t e3 = eids ? cudaMallocAsync(&bt.d_rec, bt.col_len * sizeof(uint2), s) : cudaSuccess;
-    cudaError_t e4 = cudaMallocAsync(&bt.d_erow, bt.erow_len * sizeof(uint32_t), s);
+    cudaError_t e1 = dev_malloc(&bt.d_rp, bt.rp_len * sizeof(uint32_t), s);
+    cudaError_t e2 = dev_malloc(&bt.d_col, bt.col_len * sizeof(uint32_t), s);
+    cudaError_t e3 = eids ? dev_malloc(&bt.d_rec, bt.col_len * sizeof(uint2), s) : cudaSuccess;
+    cudaError_t e4 = dev_malloc(&bt.d_erow, bt.erow_len * sizeof(uint32_t), s);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess) {
       cudaGetLastError();
       bt.release(s);
@@ -490,8 +490,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
 
   // the graph keeps its own copy of the oriented CSR: the fused task rows probe it
   {
-    cudaError_t e1 = cudaMallocAsync(&g->d_indptr, ((size_t)n + 1) * sizeof(uint32_t), s);
-    cudaError_t e2 = cudaMallocAsync(&g->d_indices, std::max<uint64_t>(m, 1) * sizeof(uint32_t) + 16, s);
+    cudaError_t e1 = dev_malloc(&g->d_indptr, ((size_t)n + 1) * sizeof(uint32_t), s);
+    cudaError_t e2 = dev_malloc(&g->d_indices, std::max<uint64_t>(m, 1) * sizeof(uint32_t) + 16, s);
     if (e1 != cudaSuccess || e2 != cudaSuccess) {
       cudaGetLastError();
       return fail(BBTC_ERR_NOMEM, "device allocation of the CSR copy failed");
@@ -576,8 +576,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   BBTC_TRY(dalloc(wflags, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(wpos, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   {
-    cudaError_t e1 = cudaMallocAsync(&g->d_words, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s);
-    cudaError_t e2 = cudaMallocAsync(&g->d_wptr, ((size_t)n + 1) * sizeof(uint32_t), s);
+    cudaError_t e1 = dev_malloc(&g->d_words, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s);
+    cudaError_t e2 = dev_malloc(&g->d_wptr, ((size_t)n + 1) * sizeof(uint32_t), s);
     if (e1 != cudaSuccess || e2 != cudaSuccess) {
       cudaGetLastError();
       return fail(BBTC_ERR_NOMEM, "device allocation of the word-compressed rows failed");
@@ -646,8 +646,9 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   return BBTC_OK;
 }
 
-int ensure_fwd(bbtc_graph* g) {
-  if (g->fwd_built) return BBTC_OK;
+namespace {
+
+int build_fwd(bbtc_graph* g) {
   bbtc_ctx* ctx = g->ctx;
   cudaStream_t s = ctx->stream;
   BBTC_CUDA(cudaSetDevice(ctx->device));
@@ -678,6 +679,20 @@ int ensure_fwd(bbtc_graph* g) {
   g->fwd_built = true;
   g->device_bytes += block_bytes(g->fwd, false);
   return BBTC_OK;
+}
+
+}  // namespace
+
+int ensure_fwd(bbtc_graph* g) {
+  if (g->fwd_built) return BBTC_OK;
+  const int rc = build_fwd(g);
+  if (rc != BBTC_OK) {
+    // a failed build (say, out of memory half way) leaves nothing behind: the
+    // frees are stream-ordered after whatever of it was enqueued
+    g->fwd.release(g->ctx->stream);
+    g->fwd = BlockTiles();
+  }
+  return rc;
 }
 
 }  // namespace bbtc

@@ -142,7 +142,7 @@ struct Buf {
 
 int balloc(Buf& b, size_t bytes, cudaStream_t s) {
   b.s = s;
-  if (cudaMallocAsync(&b.p, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
+  if (dev_malloc(&b.p, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
     cudaGetLastError();
     b.p = nullptr;
     return fail(BBTC_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
@@ -233,8 +233,8 @@ int bbtc_orient_device(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_src, const u
   }
   uint32_t* d_indptr = nullptr;
   uint32_t* d_indices = nullptr;
-  if (cudaMallocAsync(&d_indptr, ((size_t)n + 1) * 4, s) != cudaSuccess ||
-      cudaMallocAsync(&d_indices, std::max<uint64_t>(m_und, 1) * 4, s) != cudaSuccess) {
+  if (dev_malloc(&d_indptr, ((size_t)n + 1) * 4, s) != cudaSuccess ||
+      dev_malloc(&d_indices, std::max<uint64_t>(m_und, 1) * 4, s) != cudaSuccess) {
     cudaGetLastError();
     if (d_indptr) cudaFreeAsync(d_indptr, s);
     return fail(BBTC_ERR_NOMEM, "device allocation of the oriented CSR failed");

@@ -351,7 +351,7 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
     }
   }
   for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
-    if (cudaMalloc(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess ||
+    if (dev_malloc_sync(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess ||
         cudaMallocHost(&s->lanes[l].h_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess) {
       cudaGetLastError();
       rc = fail(BBTC_ERR_NOMEM, "allocation of the result slots failed");

@@ -50,6 +50,15 @@ int bbtc_last_error(char* buf, size_t len);
 /* Library version as major*10000 + minor*100 + patch. */
 int bbtc_version(void);
 
+/* Fault-injection hook for tests: the device allocation that follows `after`
+ * more successful ones fails once, as if the device were out of memory (the
+ * call that made it returns BBTC_ERR_NOMEM); after < 0 disarms.  *left (may
+ * be NULL) receives the state before the call: -1 when nothing was armed or
+ * the armed fault has fired, else the allocations it was still to let pass.
+ * BBTC_FAIL_ALLOC=k in the environment arms it when the library loads.
+ * Process-wide (all contexts and threads). */
+int bbtc_debug_fail_alloc(int64_t after, int64_t* left);
+
 /* ---- context: device, stream, scratch ------------------------------------
  * Replaces BBTc's constructor GPU set-up and PrepareGpu
  * (src/triangle_counting/bb_tc.cpp:17-33, bb_tc_helper.cpp:53-73): one

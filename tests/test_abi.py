@@ -60,6 +60,13 @@ def test_errors_are_status_codes_not_crashes():
     assert lib.bbtc_count(None, None, None, 0, -1, None, None) == -1
 
 
+def test_allocation_fault_hook_arms_and_disarms():
+    assert core.debug_fail_alloc(5) == -1
+    assert core.debug_fail_alloc(2) == 5
+    assert core.debug_fail_alloc(-1) == 2
+    assert core.debug_fail_alloc(-1) == -1
+
+
 def test_host_library_exports():
     lib = _lib.host()
     for n in ("bbtcg_rmat", "bbtcg_chung_lu", "bbtcg_rgg", "bbtcg_from_pairs", "bbtcp_cuts"):
