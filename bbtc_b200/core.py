@@ -52,7 +52,7 @@ class Opts(c.Structure):
 
 class GraphInfo(c.Structure):
     _fields_ = [("n", c.c_uint32), ("P", c.c_uint32), ("m", c.c_uint64), ("device_bytes", c.c_uint64),
-                ("layout_ms", c.c_double)]
+                ("layout_ms", c.c_double), ("zero_copy", c.c_uint32), ("reserved", c.c_uint32)]
 
 
 TASK_DTYPE = np.dtype([("ab", np.uint32), ("bc", np.uint32), ("ac", np.uint32)])
@@ -74,6 +74,7 @@ def lib() -> ctypes.CDLL:
         "bbtc_ctx_destroy": [vp],
         "bbtc_ctx_stream": [vp, c.POINTER(vp)],
         "bbtc_ctx_sm_count": [vp, c.POINTER(c.c_int)],
+        "bbtc_ctx_set_zero_copy": [vp, u64],
         "bbtc_graph_upload": [vp, u32, vp, vp, u64, vp, u32, c.POINTER(vp)],
         "bbtc_graph_upload_device": [vp, u32, vp, vp, u64, vp, u32, c.POINTER(vp)],
         "bbtc_graph_free": [vp],
@@ -163,6 +164,11 @@ class Context:
         s = c.c_void_p()
         check(lib().bbtc_ctx_stream(self.handle, c.byref(s)))
         return s.value or 0
+
+    def set_zero_copy(self, max_bytes: int) -> None:
+        """Host arrays up to max_bytes in mapped page-locked memory are read by a
+        kernel instead of the copy engines (0 turns it off)."""
+        check(lib().bbtc_ctx_set_zero_copy(self.handle, int(max_bytes)))
 
     @property
     def sm_count(self) -> int:
@@ -367,7 +373,7 @@ class BBTc:
 # ---- request server (continuous batching) ----------------------------------
 class ServerOpts(c.Structure):
     _fields_ = [("hbm_budget", c.c_uint64), ("max_batch", c.c_uint32), ("max_requests", c.c_uint32),
-                ("loaders", c.c_uint32), ("reserved", c.c_uint32), ("count", Opts),
+                ("loaders", c.c_uint32), ("copy_engine_uploads", c.c_uint32), ("count", Opts),
                 ("small_edges", c.c_uint64), ("large_blocks_per_sm", c.c_uint32), ("aging_ms", c.c_uint32),
                 ("pool_bytes", c.c_uint64)]
 
@@ -412,7 +418,7 @@ class Server:
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch: int = 0, loaders: int = 0,
                  opts: Opts | None = None, small_edges: int = 0, large_blocks_per_sm: int = 0,
-                 aging_ms: int | None = None, pool_bytes: int = 0):
+                 aging_ms: int | None = None, pool_bytes: int = 0, copy_engine_uploads: bool = False):
         L = _server_lib()
         so = ServerOpts()
         L.bbtc_server_opts_default(c.byref(so))
@@ -432,6 +438,7 @@ class Server:
             so.aging_ms = aging_ms
         if pool_bytes:
             so.pool_bytes = pool_bytes
+        so.copy_engine_uploads = 1 if copy_engine_uploads else 0
         self._h = c.c_void_p()
         check(L.bbtc_server_create(device, c.byref(so), c.byref(self._h)))
         self._keep: dict[int, tuple] = {}

@@ -220,6 +220,12 @@ int bbtc_ctx_sm_count(bbtc_ctx* ctx, int* sms) {
   return BBTC_OK;
 }
 
+int bbtc_ctx_set_zero_copy(bbtc_ctx* ctx, uint64_t max_bytes) {
+  if (!ctx) return fail(BBTC_ERR_ARG, "NULL context");
+  ctx->zero_copy_bytes = max_bytes;
+  return BBTC_OK;
+}
+
 int bbtc_graph_upload(bbtc_ctx* ctx, uint32_t n, const uint32_t* indptr, const uint32_t* indices, uint64_t m,
                       const uint32_t* cuts, uint32_t P, bbtc_graph** out) {
   if (!ctx || !out || !indptr || (m && !indices)) return fail(BBTC_ERR_ARG, "NULL argument");
@@ -268,6 +274,8 @@ int bbtc_graph_info_get(const bbtc_graph* g, bbtc_graph_info* info) {
   info->m = g->m;
   info->device_bytes = g->device_bytes;
   info->layout_ms = g->layout_ms;
+  info->zero_copy = g->zero_copy ? 1u : 0u;
+  info->reserved = 0;
   return BBTC_OK;
 }
 

@@ -145,6 +145,8 @@ struct bbtc_ctx {
   size_t smem_set = 0;                 // dynamic shared memory the count kernels are opted in to
   uint32_t layout_blocks_per_sm = 8;   // grid cap of the layout kernels (256 threads a block)
   uint32_t upload_window = 0;          // host uploads: pieces in flight at most (0 = all at once)
+  uint64_t zero_copy_bytes = 0;        // host arrays up to this size in mapped page-locked memory are read
+                                       // by a kernel instead of the copy engines (0 = never)
   // Page-locked staging for the small control copies (cut vectors, tile
   // offsets and statistics, counts).  A copy to or from pageable memory is
   // staged by the driver through buffers every thread shares, so one that
@@ -205,6 +207,7 @@ struct bbtc_graph {
   uint64_t device_bytes = 0;
   double layout_ms = 0;
   bool fwd_built = false;         // the forward block CSR is built on first use (task-list counting, tile stats)
+  bool zero_copy = false;         // the upload read the host CSR with a kernel (no copy-engine transfer)
   uint32_t last_launches = 0;
   std::map<std::string, std::unique_ptr<bbtc::Plan>> plans;  // cached queues keyed by request
 };

@@ -26,6 +26,7 @@
 // its tile by bisection of the cut vector and the first edge of every (row,
 // tile) run writes the run length, so no thread walks a whole row.
 #include <cub/cub.cuh>
+#include <cuda.h>
 
 #include <algorithm>
 #include <cstring>
@@ -57,6 +58,24 @@ __device__ __forceinline__ uint32_t lower_bound_range(const uint32_t* __restrict
     if (a[mid] < x) lo = mid + 1; else hi = mid;
   }
   return lo;
+}
+
+// Host-to-device copy done by the SMs: `src` is page-locked host memory
+// mapped into the device's address space, read over the host link, so the
+// copy does not queue behind other streams' transfers on the copy engines.
+// `dst` is a device allocation (256-byte aligned); words = bytes / 4.
+__global__ void k_copy_mapped(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint64_t words) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t done = 0;
+  if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+    const uint64_t v = words / 4;
+    const uint4* __restrict__ s4 = reinterpret_cast<const uint4*>(src);
+    uint4* __restrict__ d4 = reinterpret_cast<uint4*>(dst);
+    for (uint64_t i = t0; i < v; i += stride) d4[i] = s4[i];
+    done = v * 4;
+  }
+  for (uint64_t i = done + t0; i < words; i += stride) dst[i] = src[i];
 }
 
 // Input contract check: monotone row pointers, strictly increasing rows, ids < n.
@@ -312,6 +331,42 @@ __global__ void k_gather(const uint32_t* __restrict__ src, const uint32_t* __res
 
 inline uint64_t align4(uint64_t x) { return (x + 3) & ~3ull; }
 
+// True when [p, p + bytes) lies wholly inside one page-locked host allocation
+// (or registered range) that the current device reads at the same address.
+// Both ends are asked of the runtime, and the allocation's extent of the
+// driver; any failure, or a driver that cannot answer, means "no".
+bool mapped_host_range(const void* p, size_t bytes) {
+  if (!p || bytes == 0 || (reinterpret_cast<uintptr_t>(p) & 3)) return false;
+  const char* last = static_cast<const char*>(p) + bytes - 1;
+  for (const void* q : {p, static_cast<const void*>(last)}) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (a.type != cudaMemoryTypeHost || a.devicePointer != q) return false;
+  }
+  using GetAttr = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+  static const GetAttr get = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuPointerGetAttribute", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return static_cast<GetAttr>(nullptr);
+    }
+    return reinterpret_cast<GetAttr>(f);
+  }();
+  if (!get) return false;
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  if (get(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, (CUdeviceptr)p) != CUDA_SUCCESS ||
+      get(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, (CUdeviceptr)p) != CUDA_SUCCESS)
+    return false;
+  const uint64_t b = (uint64_t)reinterpret_cast<uintptr_t>(p);
+  return size > 0 && b >= start && b + bytes <= (uint64_t)start + size;
+}
+
 // Build one block CSR (forward or reversed) from a CSR in device memory whose
 // per-edge row ids are `rows`.  With `eids` the reversed build also writes the
 // forward-edge records.  The tile statistics land in `st` (device, 4*P*P words)
@@ -513,7 +568,17 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
       }
     } ring{evs};
     uint32_t issued = 0;
+    uint32_t by_kernel = 0;
     auto copy = [&](void* dst, const void* src, size_t bytes) -> int {
+      if (host && bytes <= ctx->zero_copy_bytes && mapped_host_range(src, bytes)) {
+        const uint64_t words = bytes / 4;
+        const uint64_t blocks = std::max<uint64_t>(1, (words + 4095) / 4096);
+        k_copy_mapped<<<(int)std::min<uint64_t>(blocks, 2ull * ctx->sms), 256, 0, s>>>(
+            static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(src), words);
+        BBTC_CUDA(cudaGetLastError());
+        by_kernel++;
+        return BBTC_OK;
+      }
       const size_t piece = host ? (size_t)8 << 20 : bytes;
       for (size_t o = 0; o < bytes; o += piece) {
         if (window) {
@@ -530,6 +595,7 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     };
     BBTC_TRY(copy(g->d_indptr, in_indptr, ((size_t)n + 1) * sizeof(uint32_t)));
     if (m) BBTC_TRY(copy(g->d_indices, in_indices, m * sizeof(uint32_t)));
+    g->zero_copy = by_kernel > 0;
   }
   const uint32_t* d_indptr = g->d_indptr;
   const uint32_t* d_indices = g->d_indices;

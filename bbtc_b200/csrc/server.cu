@@ -349,6 +349,11 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
       c->layout_blocks_per_sm = 2;
       c->upload_window = 2;
     }
+    // small requests from page-locked buffers are read by a kernel: their
+    // copies otherwise waited behind large uploads on the copy engines
+    // (p99 4.1 ms for a copy whose median is 0.03 ms)
+    if (rc == BBTC_OK && i % 2 == 0 && !s->opts.copy_engine_uploads)
+      c->zero_copy_bytes = 4 * std::max<uint64_t>(s->opts.small_edges, 1ull << 22) + 64;
   }
   for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
     if (dev_malloc_sync(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess ||

@@ -80,6 +80,8 @@ def parse():
     p.add_argument("--serve-max-scale", type=int, default=22)
     p.add_argument("--loaders", type=int, default=4, help="serve: loader threads")
     p.add_argument("--pin", type=int, default=1, help="serve: request buffers in page-locked host memory")
+    p.add_argument("--copy-engine-uploads", action="store_true",
+                   help="serve: small requests go through the copy engines even from page-locked buffers")
     p.add_argument("--trace", default="", help="serve: write every request's stage timestamps to this JSON file")
     return p.parse_args()
 
@@ -365,7 +367,7 @@ def run_serve(args):
             pool[s] = [(types.SimpleNamespace(n=g.n, m=g.m, indptr=pin(g.indptr), indices=pin(g.indices)), c)
                        for g, c in pool[s]]
     picks = [pool[int(s)][int(rng.integers(len(pool[int(s)])))] for s in scales]
-    srv = Server(0, loaders=args.loaders)
+    srv = Server(0, loaders=args.loaders, copy_engine_uploads=args.copy_engine_uploads)
     # warm-up: one request per scale
     for s in sorted(pool):
         g, c = pool[s][0]
@@ -422,7 +424,8 @@ def run_serve(args):
            "config": {"workload": f"serving: Poisson {args.rate:g} req/s for {args.duration:g} s, R-MAT scale "
                                   f"12+Geom(0.3) <= {args.serve_max_scale}, ef 16", "requests": n_req,
                       "generate_s": round(gen_s, 1), "launches": stats.launches, "max_batch": stats.max_batch,
-                      "loaders": args.loaders, "pinned_requests": bool(pinned)},
+                      "loaders": args.loaders, "pinned_requests": bool(pinned),
+                      "small_uploads": "copy engines" if args.copy_engine_uploads or not pinned else "kernel reads"},
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "p50_scale_le_18": float(np.percentile(lat18, 50)) if lat18 else None,
                           "p99_scale_le_18": float(np.percentile(lat18, 99)) if lat18 else None,

@@ -70,6 +70,14 @@ int bbtc_ctx_destroy(bbtc_ctx* ctx);
 int bbtc_ctx_stream(bbtc_ctx* ctx, void** stream);
 /* Number of SMs of the context's device. */
 int bbtc_ctx_sm_count(bbtc_ctx* ctx, int* sms);
+/* Host uploads of this context: an indptr or indices array of at most
+ * max_bytes that lies wholly in one page-locked host allocation mapped into
+ * the device's address space (cudaHostAlloc / cudaMallocHost memory, or
+ * cudaHostRegister'd ranges) is read by a kernel over the host link instead
+ * of being queued on the copy engines, where a small transfer waits behind
+ * other streams' large ones.  Anything else is copied as usual.  0 (the
+ * default) turns it off.  The server turns it on for small requests. */
+int bbtc_ctx_set_zero_copy(bbtc_ctx* ctx, uint64_t max_bytes);
 
 /* ---- graph: device-resident block CSR ------------------------------------
  * Replaces BlockCSR(cuts, x_adj, adj) + CSRtoBCSR (block_csr.cpp:35-42,
@@ -98,6 +106,8 @@ typedef struct bbtc_graph_info {
   uint64_t m;             /* oriented edges, the reference's "Number of Edges" */
   uint64_t device_bytes;  /* device memory the graph holds */
   double layout_ms;       /* device time of the layout build */
+  uint32_t zero_copy;     /* 1: the upload read the host CSR with a kernel (bbtc_ctx_set_zero_copy) */
+  uint32_t reserved;
 } bbtc_graph_info;
 int bbtc_graph_info_get(const bbtc_graph* g, bbtc_graph_info* info);
 
@@ -264,7 +274,9 @@ typedef struct bbtc_server_opts {
   uint32_t max_batch;     /* graphs per launch (0 = 4096) */
   uint32_t max_requests;  /* requests held (queued, running or finished, not released) (0 = 2^20) */
   uint32_t loaders;       /* loader threads, each with its own stream (0 = 2) */
-  uint32_t reserved;
+  uint32_t copy_engine_uploads; /* 1: small requests' CSRs always go through the copy engines; 0 (default):
+                                   from page-locked host buffers they are read by a kernel
+                                   (bbtc_ctx_set_zero_copy) */
   bbtc_opts count;        /* launch options of every batch */
   uint64_t small_edges;   /* graphs of at most this many edges use the high-priority lane (0 = 2^22) */
   uint32_t large_blocks_per_sm; /* persistent blocks per SM of the large lane (0 = 3) */

@@ -299,6 +299,40 @@ def test_device_layout_validates(ctx):
             st.free()
 
 
+def test_zero_copy_upload(ctx):
+    """A host CSR in page-locked memory read by a kernel instead of the copy
+    engines: used only when enabled, within the size limit and for mapped
+    page-locked sources; the layout and count are the same."""
+    import torch
+    g = graphs.rmat(12, 16, seed=21)
+    cuts = graphs.cuts(g, 6, "pal")
+    want = oracle.count(g.n, g.indptr, g.indices, cuts)
+    ip = torch.from_numpy(g.indptr.view(np.int32)).pin_memory()
+    ix = torch.from_numpy(g.indices.view(np.int32)).pin_memory()
+    shifted = torch.empty(g.m + 1, dtype=torch.int32, pin_memory=True)  # a start that is not 16-byte aligned
+    shifted[1:] = ix
+    try:
+        for limit, src, expect in ((0, ix.data_ptr(), 0), (64 << 20, ix.data_ptr(), 1), (1024, ix.data_ptr(), 0),
+                                   (64 << 20, shifted.data_ptr() + 4, 1)):
+            ctx.set_zero_copy(limit)
+            st = Graph.upload_ptrs(ctx, g.n, ip.data_ptr(), src, g.m, cuts)
+            try:
+                assert st.info().zero_copy == expect, (limit, expect)
+                st.validate()
+                assert st.count() == want
+            finally:
+                st.free()
+        ctx.set_zero_copy(64 << 20)
+        st = Graph.from_csr(ctx, g, cuts)  # pageable numpy arrays: copied as usual
+        try:
+            assert st.info().zero_copy == 0
+            assert st.count() == want
+        finally:
+            st.free()
+    finally:
+        ctx.set_zero_copy(0)
+
+
 @pytest.mark.parametrize("bitmap_words", [16, 64, 256])
 def test_mixed_pivot_kinds_in_one_queue(ctx, bitmap_words):
     """pal cuts give parts of very different widths, so one persistent launch

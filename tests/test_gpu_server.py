@@ -95,3 +95,36 @@ def test_autotune_sweep_and_cache(ctx, tmp_path, monkeypatch):
         assert ms2 is None and o2.bitmap_words == o.bitmap_words and o2.unit_work == o.unit_work
     finally:
         st.free()
+
+
+def _pinned(keep):
+    import torch
+
+    def pin(a):
+        t = torch.empty(max(1, a.size), dtype=torch.int32, pin_memory=True)
+        t.numpy()[:a.size] = a.view(np.int32)
+        keep.append(t)
+        return t.numpy()[:a.size].view(np.uint32)
+    return pin
+
+
+def test_pinned_requests_counted_right():
+    """Small requests in page-locked buffers are read by a kernel (no copy
+    engine); large ones, and the same graphs from pageable memory, are copied."""
+    gs = mix()
+    cuts = [graphs.cuts(g, 4 + i % 5, "uni") for i, g in enumerate(gs)]
+    want = [oracle.count(g.n, g.indptr, g.indices, c) for g, c in zip(gs, cuts)]
+    keep = []
+    pin = _pinned(keep)
+    pinned = [(pin(g.indptr), pin(g.indices)) for g in gs]
+    for small_edges in (0, 1 << 12):  # default split, and most graphs on the large (copied) lane
+        with Server(0, loaders=2, small_edges=small_edges) as srv:
+            ids = []
+            for rep in range(3):
+                for i, g in enumerate(gs):
+                    ip, ix = pinned[i] if rep != 1 else (g.indptr, g.indices)
+                    ids.append((srv.submit(g.n, ip, ix, cuts[i]), i))
+            for rid, i in ids:
+                info = srv.wait(rid, 60000)
+                assert info.status == 1 and info.count == want[i], (gs[i].name, info.status, info.count, want[i])
+                srv.release(rid)
