@@ -419,6 +419,7 @@ int bbtc_count_async(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint3
 }
 
 int bbtc_count_wait(bbtc_ctx* ctx, bbtc_graph* g, uint64_t* out) {
+  Range range("bbtc count wait");
   if (!ctx || !g || !out) return fail(BBTC_ERR_ARG, "NULL argument");
   BBTC_CUDA(cudaSetDevice(ctx->device));
   uint64_t* h = reinterpret_cast<uint64_t*>(ctx->h_stage + kStageOut);
@@ -510,6 +511,7 @@ int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bb
 }
 
 int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, const bbtc_opts* opts, uint64_t* outs) {
+  Range range("bbtc count batch");
   if (!ctx || (ng && (!graphs || !outs))) return fail(BBTC_ERR_ARG, "NULL argument");
   if (ng == 0) return BBTC_OK;
   bbtc_opts o;

@@ -1166,6 +1166,7 @@ static bbtc_opts resolve_opts(const std::vector<bbtc_graph*>& graphs, const bbtc
 int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
                   const std::vector<std::vector<bbtc_task>>& tasks, const bbtc_opts& in, bool fused,
                   uint64_t* d_outs, Plan* plan, bool reuse) {
+  Range range("bbtc count enqueue");
   cudaStream_t s = ctx->stream;
   const bbtc_opts o = resolve_opts(graphs, in, fused);
   BBTC_TRY(kernel_smem_optin(ctx, o));

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <map>
@@ -56,6 +57,15 @@ inline cudaError_t dev_malloc_sync(T** p, size_t bytes) {
   }
   return cudaMalloc(reinterpret_cast<void**>(p), bytes);
 }
+
+// A named range on the NVTX timeline (shown by nsys, filterable in ncu with
+// --nvtx); with no tool attached it costs a pointer check.
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
 
 constexpr uint32_t kMaxParts = 64;
 constexpr uint32_t kMaxDevices = 64;

@@ -524,6 +524,7 @@ DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_
 }
 
 int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_indices, bool host) {
+  Range range("bbtc upload + layout");
   bbtc_ctx* ctx = g->ctx;
   cudaStream_t s = ctx->stream;
   const uint32_t n = g->n;
@@ -715,6 +716,7 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
 namespace {
 
 int build_fwd(bbtc_graph* g) {
+  Range range("bbtc forward tiles");
   bbtc_ctx* ctx = g->ctx;
   cudaStream_t s = ctx->stream;
   BBTC_CUDA(cudaSetDevice(ctx->device));
@@ -771,6 +773,7 @@ int bbtc_graph_validate(const bbtc_graph* g) {
   static_assert(check::kNoSeg == kNoSegment, "empty-tile marker");
   if (!g) return fail(BBTC_ERR_ARG, "NULL graph");
   bbtc_ctx* ctx = g->ctx;
+  Range range("bbtc validate");
   cudaStream_t s = ctx->stream;
   BBTC_CUDA(cudaSetDevice(ctx->device));
   const uint32_t n = g->n;

@@ -199,6 +199,7 @@ using namespace bbtc;
 
 extern "C" int bbtc_cuts_device(bbtc_ctx* ctx, int kind, uint32_t n, const uint32_t* d_indptr,
                                 const uint32_t* d_indices, uint64_t m, uint32_t P, uint64_t seed, uint32_t* cuts) {
+  Range range("bbtc cuts");
   if (!ctx || !cuts) return fail(BBTC_ERR_ARG, "NULL argument");
   if (P < 1 || P > kMaxParts) return fail(BBTC_ERR_ARG, "P must be in [1, 64]");
   if (kind < 0 || kind > 2) return fail(BBTC_ERR_ARG, "kind must be 0 (uni), 1 (n1d) or 2 (pal)");

@@ -171,6 +171,7 @@ int bbtc_rmat_device(bbtc_ctx* ctx, int scale, int edge_factor, double a, double
 
 int bbtc_orient_device(bbtc_ctx* ctx, uint32_t n, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m_raw,
                        bbtc_csr_dev* out) {
+  Range range("bbtc orient");
   if (!ctx || !out || (m_raw && (!d_src || !d_dst))) return fail(BBTC_ERR_ARG, "NULL argument");
   if (n == 0xffffffffu) return fail(BBTC_ERR_ARG, "n must be below 2^32 - 1");
   *out = bbtc_csr_dev{};
