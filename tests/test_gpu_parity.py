@@ -299,6 +299,31 @@ def test_device_layout_validates(ctx):
             st.free()
 
 
+def test_relabelling_and_orientation_invariance(ctx):
+    """Relabelled vertices (re-oriented by degree) and an orientation by id
+    instead of degree count the same triangles on every kernel and mode."""
+    def id_oriented(n, a, b):  # smaller id -> larger id
+        lo, hi = np.minimum(a, b), np.maximum(a, b)
+        order = np.lexsort((hi, lo))
+        lo, hi = lo[order], hi[order]
+        indptr = np.concatenate([[0], np.cumsum(np.bincount(lo, minlength=n))]).astype(np.uint32)
+        return graphs.OrientedCSR(n, indptr, hi.astype(np.uint32))
+
+    g = graphs.rmat(12, 16, seed=13)
+    want = oracle.count(g.n, g.indptr, g.indices, graphs.cuts(g, 4, "uni"))
+    src = np.repeat(np.arange(g.n), np.diff(g.indptr.astype(np.int64)))
+    dst = g.indices.astype(np.int64)
+    rng = np.random.default_rng(5)
+    perm = rng.permutation(g.n)
+    relabelled = graphs.from_pairs(g.n, perm[src], perm[dst])
+    perm = rng.permutation(g.n)
+    by_id = id_oriented(g.n, perm[src], perm[dst])
+    for h, part, P in ((relabelled, "pal", 7), (by_id, "uni", 5), (by_id, "n1d", 9)):
+        cuts = graphs.cuts(h, P, part)
+        for kernel, mode in KERNEL_MODES:
+            assert gpu_count(ctx, h, cuts, kernel=kernel, mode=mode) == want, (part, kernel, mode)
+
+
 def test_zero_copy_upload(ctx):
     """A host CSR in page-locked memory read by a kernel instead of the copy
     engines: used only when enabled, within the size limit and for mapped

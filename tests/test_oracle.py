@@ -71,6 +71,35 @@ def test_partition_invariance():
     assert len(counts) == 1
 
 
+def id_oriented(n, src, dst):
+    """CSR oriented from the smaller to the larger id (not by degree)."""
+    lo, hi = np.minimum(src, dst).astype(np.int64), np.maximum(src, dst).astype(np.int64)
+    order = np.lexsort((hi, lo))
+    lo, hi = lo[order], hi[order]
+    indptr = np.concatenate([[0], np.cumsum(np.bincount(lo, minlength=n))]).astype(np.uint32)
+    return graphs.OrientedCSR(n, indptr, hi.astype(np.uint32))
+
+
+def test_relabelling_and_orientation_invariance():
+    """Relabelled vertices (re-oriented by degree) and an orientation by id
+    instead of degree give the same count: every acyclic orientation counts
+    each triangle once."""
+    g = graphs.rmat(11, 16, seed=13)
+    want = oracle.count(g.n, g.indptr, g.indices, graphs.cuts(g, 4, "uni"))
+    src = np.repeat(np.arange(g.n), np.diff(g.indptr.astype(np.int64)))
+    dst = g.indices.astype(np.int64)
+    rng = np.random.default_rng(5)
+    for _ in range(2):
+        perm = rng.permutation(g.n)
+        h = graphs.from_pairs(g.n, perm[src], perm[dst])
+        assert h.m == g.m
+        assert oracle.count(h.n, h.indptr, h.indices, graphs.cuts(h, 5, "pal")) == want
+    perm = rng.permutation(g.n)
+    h = id_oriented(g.n, perm[src], perm[dst])
+    assert h.m == g.m
+    assert oracle.count(h.n, h.indptr, h.indices, graphs.cuts(h, 3, "uni")) == want
+
+
 def test_plants_are_caught():
     """A planted mistake in the oracle's input changes the count (the check has teeth)."""
     g = graphs.rmat(10, 16, seed=5)
