@@ -26,7 +26,10 @@ int fail(int status, const std::string& msg) {
 // the next one; -1 is disarmed.
 static std::atomic<int64_t> g_alloc_fault{[] {
   const char* v = std::getenv("BBTC_FAIL_ALLOC");
-  return v && *v ? (int64_t)std::strtoll(v, nullptr, 10) : (int64_t)-1;
+  if (!v || !*v) return (int64_t)-1;
+  char* end = nullptr;
+  const long long k = std::strtoll(v, &end, 10);
+  return *end == '\0' && k >= 0 ? (int64_t)k : (int64_t)-1;  // anything but a count leaves it disarmed
 }()};
 
 bool take_alloc_fault() {

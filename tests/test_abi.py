@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from bbtc_b200 import _lib, core
 
@@ -65,6 +66,17 @@ def test_allocation_fault_hook_arms_and_disarms():
     assert core.debug_fail_alloc(2) == 5
     assert core.debug_fail_alloc(-1) == 2
     assert core.debug_fail_alloc(-1) == -1
+
+
+@pytest.mark.parametrize("value,armed", [("3", 3), ("0", 0), ("abc", -1), ("-2", -1), ("", -1)])
+def test_allocation_fault_hook_from_the_environment(value, armed):
+    import subprocess
+    import sys
+    code = "from bbtc_b200 import core; print(core.debug_fail_alloc(-1))"
+    env = dict(os.environ, BBTC_FAIL_ALLOC=value)
+    out = subprocess.run([sys.executable, "-c", code], env=env, cwd=ROOT, capture_output=True, text=True,
+                         timeout=120, check=True).stdout
+    assert int(out.strip()) == armed
 
 
 def test_host_library_exports():
