@@ -6,9 +6,10 @@
 //   loader threads: take a pending request whose estimated device footprint
 //     fits the HBM budget -- the smallest, or the oldest once it has waited
 //     aging_ms -- build its device block CSR (upload + layout) on the
-//     loader's stream for its size class (small: highest priority; large:
-//     lowest priority, layout grids capped at 2 blocks per SM, at most two
-//     8 MiB upload pieces queued at a time), and queue it on its size
+//     loader's stream for its size class (small: highest priority, a CSR in
+//     page-locked host memory read by a kernel rather than the copy
+//     engines; large: lowest priority, layout grids capped at 2 blocks per
+//     SM, at most two 8 MiB upload pieces queued at a time), and queue it on its size
 //     class's lane.  A request that could never fit fails with
 //     BBTC_ERR_CAPACITY.  With two or more loaders half of them take small
 //     requests only.
