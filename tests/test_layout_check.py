@@ -74,6 +74,20 @@ def test_empty_parts_and_phantom_rows(harness):
     assert run(exe, graph_file(d, g, cuts, "e.bin"), "none") == "OK"
 
 
+def test_edgeless_and_id_oriented_layouts_pass(harness):
+    exe, d = harness
+    empty = graphs.from_pairs(10, [], [])
+    assert run(exe, graph_file(d, empty, [0, 3, 7, 10], "z.bin"), "none") == "OK"
+    # rows oriented by id (long rows, not degree ordered): the format does not depend on the orientation
+    g = graphs.rmat(8, 16, seed=6)
+    src = np.repeat(np.arange(g.n), np.diff(g.indptr.astype(np.int64)))
+    lo, hi = np.minimum(src, g.indices), np.maximum(src, g.indices)
+    order = np.lexsort((hi, lo))
+    indptr = np.concatenate([[0], np.cumsum(np.bincount(lo[order], minlength=g.n))]).astype(np.uint32)
+    h = graphs.OrientedCSR(g.n, indptr, hi[order].astype(np.uint32))
+    assert run(exe, graph_file(d, h, graphs.cuts(h, 5, "uni"), "h.bin"), "none") == "OK"
+
+
 @pytest.mark.parametrize("fault", sorted(FAULTS))
 def test_planted_faults_are_named(harness, fault):
     exe, d = harness
