@@ -79,6 +79,35 @@ def test_allocation_fault_hook_from_the_environment(value, armed):
     assert int(out.strip()) == armed
 
 
+def test_cpp_mirror_reports_errors_as_exceptions(tmp_path):
+    """include/bbtc.hpp (the reference's class names over the C ABI) turns a
+    failing call into bbtc::Error with the status, where the reference would
+    crash: here, a context on a machine without a usable GPU, and a task list
+    for P outside [1, 64]."""
+    import shutil
+    import subprocess
+    src = tmp_path / "mirror.cpp"
+    src.write_text(r"""
+#include <cstdio>
+#include "bbtc.hpp"
+int main() {
+  int ctx_status = 0, list_status = 0;
+  try { bbtc::Context ctx(0); } catch (const bbtc::Error& e) { ctx_status = e.status(); }
+  try { bbtc::tasks::TaskList(65); } catch (const bbtc::Error& e) { list_status = e.status(); }
+  std::printf("%d %d %zu\n", ctx_status, list_status, bbtc::tasks::TaskList(4).size());
+  return 0;
+}
+""")
+    exe = tmp_path / "mirror"
+    cxx = shutil.which("g++") or shutil.which("c++")
+    subprocess.run([cxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", _lib.LIBDIR, "-lbbtc", "-Wl,-rpath," + _lib.LIBDIR], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, timeout=120).stdout.split()
+    ctx_status, list_status, n4 = (int(x) for x in out)
+    assert ctx_status in (0, -6)  # -6: no usable device here; 0 where a B200 is present
+    assert list_status == -1 and n4 == 20
+
+
 def test_host_library_exports():
     lib = _lib.host()
     for n in ("bbtcg_rmat", "bbtcg_chung_lu", "bbtcg_rgg", "bbtcg_from_pairs", "bbtcp_cuts"):
