@@ -118,9 +118,10 @@ def write_edge_list(path: str, n: int, indptr, indices) -> None:
 
 
 def ref_cli(n: int, indptr, indices, partitioner: str = "pal", ncut: int = 8, nthreads: int = 0,
-            extra: tuple[str, ...] = ()) -> dict:
+            extra: tuple[str, ...] = (), text: str | None = None) -> dict:
     """Run the reference's unmodified CPU executable on the graph written as an
-    edge list; returns the parsed output fields.  The border stays at the CPU
+    edge list (or on `text`, a graph file's contents, read by the reference's
+    own reader); returns the parsed output fields.  The border stays at the CPU
     build's default 0: `--border -1` sets Separator = |T| (src/bbtc.cpp:139-141),
     which leaves no task for the CPU workers (bb_tc.cpp:187-196) and prints 0."""
     exe = os.path.join(HERE, "_ref", "bbtc_cpu")
@@ -128,7 +129,11 @@ def ref_cli(n: int, indptr, indices, partitioner: str = "pal", ncut: int = 8, nt
         raise FileNotFoundError(exe)
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "g.el")
-        write_edge_list(path, n, indptr, indices)
+        if text is None:
+            write_edge_list(path, n, indptr, indices)
+        else:
+            with open(path, "w") as f:
+                f.write(text)
         env = dict(os.environ)
         if nthreads > 0:
             env["OMP_NUM_THREADS"] = str(nthreads)

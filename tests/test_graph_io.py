@@ -103,3 +103,37 @@ def test_malformed_text_is_refused(tmp_path, text, name):
 
 def test_missing_file(tmp_path):
     assert read(tmp_path / "none.el")[0] == -1
+
+
+def test_text_reader_agrees_with_the_reference_reader(tmp_path):
+    """A messy edge list (random directions, pairs given both ways, self loops,
+    comments, weight columns) read by this reader and by the reference's
+    unmodified executable: the same edge count and triangle count.  (Lines
+    repeated verbatim are left out: the reference keeps them as parallel
+    edges, PIGO pigo/impl/csr.impl.hpp:51, this reader drops them.)"""
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(3)
+    g = graphs.rmat(10, 8, seed=9)
+    src = np.repeat(np.arange(g.n), np.diff(g.indptr.astype(np.int64)))
+    lines = []
+    for u, v in zip(src.tolist(), g.indices.tolist()):
+        if rng.random() < 0.5:
+            u, v = v, u
+        lines.append(f"{u} {v}" + (f" {int(rng.integers(1, 9))}" if rng.random() < 0.3 else ""))
+        if rng.random() < 0.2:
+            lines.append(f"{v} {u}")
+    lines += [f"{s} {s}" for s in rng.integers(0, g.n, 20).tolist()]
+    rng.shuffle(lines)
+    text = "# comment\n% another comment\n" + "\n".join(lines) + "\n"
+    p = tmp_path / "messy.el"
+    p.write_text(text)
+    rc, kind, indptr, indices = read(p)
+    assert rc == 0 and kind == 0 and len(indices) == g.m
+    n = len(indptr) - 1
+    cuts = graphs.cuts(graphs.OrientedCSR(n, indptr, indices), 4, "pal")
+    ours = oracle.count(n, indptr, indices, cuts)
+    ref = oracle.ref_cli(0, None, None, "pal", 4, text=text)
+    assert ref["edges"] == len(indices)
+    assert ref["triangles"] == ours == oracle.count(g.n, g.indptr, g.indices, graphs.cuts(g, 4, "pal"))
