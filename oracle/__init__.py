@@ -118,7 +118,7 @@ def write_edge_list(path: str, n: int, indptr, indices) -> None:
 
 
 def ref_cli(n: int, indptr, indices, partitioner: str = "pal", ncut: int = 8, nthreads: int = 0,
-            extra: tuple[str, ...] = (), text: str | None = None) -> dict:
+            extra: tuple[str, ...] = (), text: str | None = None, suffix: str = ".el") -> dict:
     """Run the reference's unmodified CPU executable on the graph written as an
     edge list (or on `text`, a graph file's contents, read by the reference's
     own reader); returns the parsed output fields.  The border stays at the CPU
@@ -128,7 +128,7 @@ def ref_cli(n: int, indptr, indices, partitioner: str = "pal", ncut: int = 8, nt
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     with tempfile.TemporaryDirectory() as d:
-        path = os.path.join(d, "g.el")
+        path = os.path.join(d, "g" + suffix)
         if text is None:
             write_edge_list(path, n, indptr, indices)
         else:

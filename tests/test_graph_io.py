@@ -137,3 +137,23 @@ def test_text_reader_agrees_with_the_reference_reader(tmp_path):
     ref = oracle.ref_cli(0, None, None, "pal", 4, text=text)
     assert ref["edges"] == len(indices)
     assert ref["triangles"] == ours == oracle.count(g.n, g.indptr, g.indices, graphs.cuts(g, 4, "pal"))
+
+
+def test_matrix_market_agrees_with_the_reference_reader(tmp_path):
+    """A MatrixMarket coordinate file (1-based ids kept, so vertex 0 is
+    isolated; a value column) read by both readers."""
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    g = graphs.rmat(9, 16, seed=4)
+    src = np.repeat(np.arange(g.n), np.diff(g.indptr.astype(np.int64)))
+    body = "\n".join(f"{v + 1} {u + 1} 1.0" for u, v in zip(src.tolist(), g.indices.tolist()))
+    text = (f"%%MatrixMarket matrix coordinate real symmetric\n% comment\n{g.n} {g.n} {g.m}\n" + body + "\n")
+    p = tmp_path / "g.mtx"
+    p.write_text(text)
+    rc, kind, indptr, indices = read(p)
+    assert rc == 0 and kind == 1 and len(indices) == g.m
+    n = len(indptr) - 1
+    ours = oracle.count(n, indptr, indices, graphs.cuts(graphs.OrientedCSR(n, indptr, indices), 4, "uni"))
+    ref = oracle.ref_cli(0, None, None, "uni", 4, text=text, suffix=".mtx")
+    assert ref["edges"] == len(indices) and ref["triangles"] == ours
