@@ -157,3 +157,37 @@ def test_matrix_market_agrees_with_the_reference_reader(tmp_path):
     ours = oracle.count(n, indptr, indices, graphs.cuts(graphs.OrientedCSR(n, indptr, indices), 4, "uni"))
     ref = oracle.ref_cli(0, None, None, "uni", 4, text=text, suffix=".mtx")
     assert ref["edges"] == len(indices) and ref["triangles"] == ours
+
+
+def test_bbtc_caches_cross_load_with_the_reference(tmp_path):
+    """A `.bbtc` cache the reference's executable writes loads here (its valid
+    oriented CSR passes the reader's contract check), and one written here
+    loads in the reference's executable: same edges and triangles both ways."""
+    import os
+    import shutil
+    import subprocess
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    exe = os.path.join(oracle.HERE, "_ref", "bbtc_cpu")
+    g = graphs.rmat(11, 16, seed=6)
+    want = oracle.count(g.n, g.indptr, g.indices, graphs.cuts(g, 4, "uni"))
+    # reference -> here
+    path = str(tmp_path / "h.el")
+    oracle.write_edge_list(path, g.n, g.indptr, g.indices)
+    subprocess.run([exe, "--graph", path, "--ncut", "4", "--repeat", "1"], capture_output=True, text=True,
+                   timeout=300, check=True)
+    theirs = tmp_path / "theirs.bbtc"
+    shutil.copy(path + ".bbtc", theirs)
+    rc, kind, indptr, indices = read(theirs)
+    assert rc == 0 and kind == 2 and len(indices) == g.m
+    n = len(indptr) - 1
+    assert oracle.count(n, indptr, indices, graphs.cuts(graphs.OrientedCSR(n, indptr, indices), 3, "uni")) == want
+    # here -> reference
+    ours = tmp_path / "ours.bbtc"
+    assert lib().bbtcio_write_bbtc(str(ours).encode(), g.n, g.indptr.ctypes.data, g.indices.ctypes.data, g.m) == 0
+    out = subprocess.run([exe, "--graph", str(ours), "--ncut", "5", "--repeat", "1"], capture_output=True,
+                         text=True, timeout=300, check=True).stdout
+    import re
+    assert int(re.search(r"Number of Triangles: (\d+)", out).group(1)) == want
+    assert int(re.search(r"Number of Edges: (\d+)", out).group(1)) == g.m
