@@ -1068,7 +1068,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
   uint64_t total = 0;
   for (uint32_t q : order) {
     const DevTask& d = list[q];
-    total += (d.rows.nnz + d.unit_edges - 1) / d.unit_edges;
+    total += ((uint64_t)d.rows.nnz + d.unit_edges - 1) / d.unit_edges;  // 64-bit: nnz may be near 2^32
     if (total >= 0xffffffffull) return fail(BBTC_ERR_UNSUPPORTED, "more than 2^32 work units in one request");
     plan->tasks.push_back(d);
     plan->prefix.push_back((uint32_t)total);

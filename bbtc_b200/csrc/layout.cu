@@ -231,7 +231,8 @@ __global__ void k_row_index(const uint32_t* __restrict__ rp, const uint64_t* __r
   uint32_t* __restrict__ er = erow + col_off[t] / 32 + t;
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < H; b += gridDim.x * blockDim.x) {
     const uint32_t s = r[b], e = r[b + 1];
-    for (uint32_t q = (s + 31) & ~31u; q < e; q += 32) er[q >> 5] = b;
+    // 64-bit: rounding s up to a multiple of 32 must not wrap near 2^32
+    for (uint64_t q = ((uint64_t)s + 31) & ~31ull; q < e; q += 32) er[q >> 5] = b;
   }
 }
 
