@@ -70,6 +70,7 @@ def lib() -> ctypes.CDLL:
         "bbtc_last_error": [c.c_char_p, c.c_size_t],
         "bbtc_version": [],
         "bbtc_debug_fail_alloc": [c.c_int64, c.POINTER(c.c_int64)],
+        "bbtc_debug_stage_timeout": [vp, u32],
         "bbtc_ctx_create": [c.c_int, c.POINTER(vp)],
         "bbtc_ctx_destroy": [vp],
         "bbtc_ctx_stream": [vp, c.POINTER(vp)],
@@ -169,6 +170,12 @@ class Context:
         """Host arrays up to max_bytes in mapped page-locked memory are read by a
         kernel instead of the copy engines (0 turns it off)."""
         check(lib().bbtc_ctx_set_zero_copy(self.handle, int(max_bytes)))
+
+    def debug_stage_timeout(self, polls: int) -> None:
+        """Test hook: with polls > 0 the per-task kernels' staging copies are
+        not issued and each staging wait gives up after `polls` polls, so a
+        count that stages returns BBTC_ERR_TIMEOUT; 0 restores normal staging."""
+        check(lib().bbtc_debug_stage_timeout(self.handle, int(polls)))
 
     @property
     def sm_count(self) -> int:

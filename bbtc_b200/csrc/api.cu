@@ -149,6 +149,12 @@ int bbtc_debug_fail_alloc(int64_t after, int64_t* left) {
   return BBTC_OK;
 }
 
+int bbtc_debug_stage_timeout(bbtc_ctx* ctx, uint32_t polls) {
+  if (!ctx) return bbtc::fail(BBTC_ERR_ARG, "NULL context");
+  ctx->debug_stage_polls = polls;
+  return BBTC_OK;
+}
+
 int bbtc_ctx_create(int device, bbtc_ctx** out) {
   if (!out) return fail(BBTC_ERR_ARG, "out is NULL");
   *out = nullptr;

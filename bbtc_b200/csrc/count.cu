@@ -18,9 +18,10 @@
 //
 // Fused task rows (persistent form over the whole task list): the tasks
 // (i, j, k) for all k >= j share their ab tile, and their sum over k is
-// sum_{(u, v) in ab} |N+(u) ∩ N+(v)| with every common neighbour w > v.  One
-// pass over the reversed tile (j, i) takes it: per pivot v the whole row N+(v)
-// is the structure, and per in-edge (u, v) the ids of N+(u) after v are
+// sum_{(u, v) in ab} |N+(u) ∩ N+(v) ∩ [cuts[j], ∞)|.  One pass over the
+// reversed tile (j, i) takes it: per pivot v the row N+(v) from cuts[j] on
+// (for a CSR oriented from lower to higher ids, the whole row) is the
+// structure, and per in-edge (u, v) the ids of N+(u) that can meet it are
 // streamed -- their range is stored with the in-edge, so no row pointer is
 // chased.  This visits each edge once instead of once per k.
 //
@@ -48,7 +49,7 @@ namespace {
 
 constexpr uint32_t FULL = 0xffffffffu;
 // per warp after its bitmap: 33 segment starts, 32 bases, a pad word and the
-// 8-byte aligned FusedFrame (22 words), rounded up to an even count
+// 8-byte aligned FusedFrame (28 words), rounded up to an even count
 constexpr uint32_t kSegWords = 96;
 constexpr uint32_t kFrameOffset = 66;  // words after the bitmap
 // per-warp bulk-staging state of the per-task kernels, after the bitmap:
@@ -58,6 +59,8 @@ constexpr uint32_t kPhaseOffset = 94;
 constexpr uint32_t kStageOffFlag = 95;
 constexpr uint32_t kStageMin = 64;         // pivot rows this long or longer are staged by one bulk copy
 constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait polls before a staging copy is given up
+// values of the warp's staging flag (state[kStageOffFlag])
+constexpr uint32_t kStageOn = 0, kStageOff = 1, kStageDead = 2;
 constexpr uint32_t kSplitList = 128; // split pivots: room for the ids below the bitmap window
 
 // ---- bulk copies into shared memory (cp.async.bulk + mbarrier) ------------
@@ -82,18 +85,23 @@ __device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, uint3
 }
 
 // Wait for the phase with parity `parity` of `bar` to complete; false when
-// it has not after kWaitLimit polls.
-__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kWaitLimit; i++) {
+// it has not after `limit` polls.  Warp-uniform: true only when every lane
+// saw the phase complete (each lane's own wait orders its later reads).
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+  bool done_all = false;
+  for (uint32_t i = 0; i < limit; i++) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(done)
         : "r"(smem_addr(bar)), "r"(parity)
         : "memory");
-    if (done) return true;
+    if (done) {
+      done_all = true;
+      break;
+    }
   }
-  return false;
+  return __all_sync(FULL, done_all);
 }
 
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t x) {
@@ -415,14 +423,22 @@ __device__ __forceinline__ uint32_t next_row(const uint32_t* __restrict__ rp, ui
 // row itself (pivot_pass).  The column segment of a tile starts on a 16-byte
 // boundary and the pool ends with a 16-byte tail, so the rounded span stays
 // inside the allocation.
+//
+// A copy that has not landed after the wait limit voids the count (the
+// error word; the host fails the call with BBTC_ERR_TIMEOUT).  The warp then
+// waits once more, bounded, for the copy still in flight: if it lands, the
+// staged span is cleared and the warp goes on without staging; if not, the
+// warp may not touch its buffer again and stops (kStageDead), taking no more
+// work.  `dbg` > 0 is the test hook of bbtc_debug_stage_timeout: no copy is
+// issued, so the wait gives up after `dbg` polls with nothing in flight.
 template <uint32_t KIND>
 __device__ __forceinline__ bool staged_pass(const uint32_t* __restrict__ tile_col, uint32_t ps, uint32_t pd,
                                             uint32_t words, const TileSegs& segs, uint32_t e, uint32_t ee,
                                             const uint32_t* __restrict__ prb_col, uint32_t* bm, uint32_t bm_words,
                                             uint32_t* sstart, uint32_t* sbase, uint32_t lane, uint32_t* err,
-                                            unsigned long long& acc) {
+                                            uint32_t dbg, unsigned long long& acc) {
   uint32_t* state = bm + bm_words;
-  if (pd < kStageMin || state[kStageOffFlag]) return false;
+  if (pd < kStageMin || state[kStageOffFlag] != kStageOn) return false;
   const uint32_t a0 = ps & ~3u, off = ps & 3u;
   const uint32_t span = ((ps + pd + 3u) & ~3u) - a0;  // words, a multiple of 4
   // bitmap kind: after the bitmap and its always-zero word; list kind: the list itself
@@ -430,15 +446,22 @@ __device__ __forceinline__ bool staged_pass(const uint32_t* __restrict__ tile_co
   if (span > bm_words - (uint32_t)(stage - bm)) return false;
   uint64_t* bar = reinterpret_cast<uint64_t*>(state + kBarOffset);
   const uint32_t phase = state[kPhaseOffset];
-  if (lane == 0) bulk_to_shared(stage, tile_col + a0, span * 4u, bar);
-  const bool ok = bar_wait(bar, phase);
+  const uint32_t limit = dbg ? dbg : kWaitLimit;
+  if (lane == 0 && !dbg) bulk_to_shared(stage, tile_col + a0, span * 4u, bar);
+  const bool ok = bar_wait(bar, phase, limit);
   __syncwarp();
   if (!ok) {
-    // the copy did not land in time: the count is void (the host sees the
-    // flag and fails the call), and this warp stages nothing more
-    if (lane == 0) {
-      atomicOr(err, 1u);
-      state[kStageOffFlag] = 1u;
+    // the copy did not land in time: the count is void
+    if (lane == 0) atomicOr(err, 1u);
+    const bool landed = bar_wait(bar, phase, limit);  // drain the copy still in flight
+    if (landed) {
+      for (uint32_t i = lane; i < span; i += 32) stage[i] = 0;
+      if (lane == 0) {
+        state[kPhaseOffset] = phase ^ 1u;
+        state[kStageOffFlag] = kStageOff;
+      }
+    } else if (lane == 0) {
+      state[kStageOffFlag] = kStageDead;
     }
     __syncwarp();
     return true;
@@ -485,14 +508,20 @@ __device__ __forceinline__ void staging_init(uint32_t* bm, uint32_t bm_words, ui
   if (lane == 0) {
     bar_init(reinterpret_cast<uint64_t*>(state + kBarOffset));
     state[kPhaseOffset] = 0;
-    state[kStageOffFlag] = 0;
+    state[kStageOffFlag] = kStageOn;
   }
   __syncwarp();
 }
 
+// True once a staging copy of this warp was given up while possibly still in
+// flight: the warp stops working (its count is void already).
+__device__ __forceinline__ bool staging_dead(const uint32_t* bm, uint32_t bm_words) {
+  return bm[bm_words + kStageOffFlag] == kStageDead;
+}
+
 __device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
                                                      uint32_t* sstart, uint32_t* sbase, uint32_t lane,
-                                                     uint32_t bm_words, uint32_t* err) {
+                                                     uint32_t bm_words, uint32_t* err, uint32_t dbg) {
   const uint32_t* __restrict__ r_rp = tk.rows.rp;
   const uint32_t* __restrict__ p_rp = tk.pivot.rp;
   const uint32_t* __restrict__ p_col = tk.pivot.col;
@@ -513,23 +542,58 @@ __device__ __noinline__ unsigned long long task_unit(const DevTask& tk, uint32_t
       switch (tk.kind) {
         case kPivotBitmap:
           if (!staged_pass<kPivotBitmap>(p_col, ps, pd, tk.words, segs, e, ee, tk.probe.col, bm, bm_words, sstart,
-                                         sbase, lane, err, acc))
+                                         sbase, lane, err, dbg, acc))
             acc += pivot_pass<kPivotBitmap, false>(prow, pd, 0, tk.words, 0, segs, e, ee, tk.probe.col, bm, sstart,
                                                    sbase, lane);
           break;
         case kPivotList:
           if (!staged_pass<kPivotList>(p_col, ps, pd, 0, segs, e, ee, tk.probe.col, bm, bm_words, sstart, sbase, lane,
-                                       err, acc))
+                                       err, dbg, acc))
             acc += pivot_pass<kPivotList, false>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
           break;
         default:
           acc += pivot_pass<kPivotGlobal, false>(prow, pd, 0, 0, 0, segs, e, ee, tk.probe.col, bm, sstart, sbase, lane);
       }
+      if (staging_dead(bm, bm_words)) return acc;
     }
     e = ee;
     if (e < e1) b = next_row(r_rp, H, b, e, lane);
   }
   return acc;
+}
+
+// The pivot of a fused task row (i, j): the tasks (i, j, k >= j) count the
+// common neighbours w of an in-edge (u, v) with w in column parts k >= j,
+// i.e. w >= lo = cuts[j] (the reference's tiles ac = (i, k), bc = (j, k),
+// src/triangle_counting/gpu_sparse_kernel.cu:25-46).  Drops the ids of
+// N+(v) below lo from the pivot row [ps, ps + pd) and from its word pairs
+// [ws, ws + wn); mask0 clears the dropped ids that share the first kept
+// pair's word.  Called only when N+(v) starts below lo, which a CSR oriented
+// from lower to higher ids never does (every id of N+(v) exceeds v >= lo).
+__device__ __noinline__ void pivot_suffix(const uint32_t* __restrict__ gi, const uint2* __restrict__ gw, uint32_t lo,
+                                          uint32_t& ps, uint32_t& pd, uint32_t& ws, uint32_t& wn, uint32_t& mask0) {
+  const uint32_t k = lower_bound_u32(gi + ps, pd, lo);
+  ps += k;
+  pd -= k;
+  if (pd == 0) {
+    wn = 0;
+    return;
+  }
+  const uint32_t first = gi[ps];
+  // first pair whose word holds `first` (a row's pair words strictly increase)
+  uint32_t lo_p = 0, n = wn;
+  while (n > 0) {
+    const uint32_t half = n >> 1;
+    if (gw[ws + lo_p + half].x < (first >> 5)) {
+      lo_p += half + 1;
+      n -= half + 1;
+    } else {
+      n = half;
+    }
+  }
+  ws += lo_p;
+  wn -= lo_p;
+  mask0 = FULL << (first & 31);
 }
 
 // One fused task-row unit: in-edges [unit*K, ...) of the reversed tile (j, i).
@@ -550,8 +614,14 @@ __device__ __noinline__ unsigned long long fused_unit(const DevTask& tk, uint32_
   while (e < e1) {
     const uint32_t ee = min(r_rp[b + 1], e1);
     const uint32_t v = tk.pivot_base + b;
-    const uint32_t ps = gp[v];
-    const uint32_t pd = gp[v + 1] - ps;
+    uint32_t ps = gp[v];
+    uint32_t pd = gp[v + 1] - ps;
+    if (pd > 0 && gi[ps] < tk.pivot_base) {
+      // keep the ids in the task columns only (this pivot is built from ids)
+      const uint32_t k = lower_bound_u32(gi + ps, pd, tk.pivot_base);
+      ps += k;
+      pd -= k;
+    }
     if (pd > 0) {
       const uint32_t* prow = gi + ps;
       const uint32_t first = prow[0];
@@ -591,9 +661,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 
 __device__ __forceinline__ unsigned long long dispatch_unit(const DevTask& tk, uint32_t unit, uint32_t* bm,
                                                             uint32_t* sstart, uint32_t* sbase, uint32_t lane,
-                                                            uint32_t bm_words, uint32_t* err) {
+                                                            uint32_t bm_words, uint32_t* err, uint32_t dbg) {
   if (tk.kind == kFusedRow) return fused_unit(tk, unit, bm, sstart, sbase, lane, bm_words);
-  return task_unit(tk, unit, bm, sstart, sbase, lane, bm_words, err);
+  return task_unit(tk, unit, bm, sstart, sbase, lane, bm_words, err, dbg);
 }
 
 // Persistent form: every warp claims units from one head until the queue is
@@ -602,7 +672,8 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_count_queue(const DevTask* __restrict__ tasks,
                                                         const uint32_t* __restrict__ prefix, uint32_t ntasks,
                                                         uint32_t total_units, uint32_t* __restrict__ head,
-                                                        unsigned long long* __restrict__ outs, uint32_t bm_words) {
+                                                        unsigned long long* __restrict__ outs, uint32_t bm_words,
+                                                        uint32_t dbg) {
   extern __shared__ __align__(16) uint32_t sh[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
@@ -623,15 +694,16 @@ __global__ void __launch_bounds__(256, MINB) k_count_queue(const DevTask* __rest
     }
     const DevTask& tk = tasks[lo];
     const unsigned long long c =
-        warp_sum(dispatch_unit(tk, g - prefix[lo], bm, sstart, sbase, lane, bm_words, err));
+        warp_sum(dispatch_unit(tk, g - prefix[lo], bm, sstart, sbase, lane, bm_words, err, dbg));
     if (lane == 0 && c) atomicAdd(&outs[tk.slot], c);
+    if (staging_dead(bm, bm_words)) break;
   }
 }
 
 // Plain form: one task per launch; warps stride over the task's units.
 __global__ void __launch_bounds__(256, 4) k_count_task(const DevTask* __restrict__ task, uint32_t units,
                                                        unsigned long long* __restrict__ outs, uint32_t bm_words,
-                                                       uint32_t* __restrict__ err) {
+                                                       uint32_t* __restrict__ err, uint32_t dbg) {
   extern __shared__ __align__(16) uint32_t sh[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* bm = sh + warp * (bm_words + kSegWords);
@@ -642,8 +714,10 @@ __global__ void __launch_bounds__(256, 4) k_count_task(const DevTask* __restrict
   const DevTask& tk = *task;
   const uint32_t wpb = blockDim.x >> 5;
   unsigned long long acc = 0;
-  for (uint32_t u = blockIdx.x * wpb + warp; u < units; u += gridDim.x * wpb)
-    acc += dispatch_unit(tk, u, bm, sstart, sbase, lane, bm_words, err);
+  for (uint32_t u = blockIdx.x * wpb + warp; u < units; u += gridDim.x * wpb) {
+    acc += dispatch_unit(tk, u, bm, sstart, sbase, lane, bm_words, err, dbg);
+    if (staging_dead(bm, bm_words)) break;
+  }
   acc = warp_sum(acc);
   if (lane == 0 && acc) atomicAdd(&outs[tk.slot], acc);
 }
@@ -665,6 +739,7 @@ struct FusedFrame {
   uint32_t H, e1, b, ee; // rows, unit end, current row, end of the current row's entries
   uint32_t pivot_base, ps, pd, base, words, rlen, kind, slot;
   uint32_t ws, wn;       // the pivot row's word pairs
+  uint32_t mask0;        // bits kept of the first pair (pivot_suffix)
 };
 static_assert(sizeof(FusedFrame) <= (kSegWords - kFrameOffset) * sizeof(uint32_t), "frame does not fit");
 
@@ -735,10 +810,10 @@ __device__ __forceinline__ void fused_build(const uint32_t* __restrict__ prow, u
 // share.  Split kind: only the words of its window (w >= base_w).
 template <uint32_t KIND>
 __device__ __forceinline__ void fused_build_words(const uint2* __restrict__ pw, uint32_t wn, uint32_t base_w,
-                                                  uint32_t* bm, uint32_t lane) {
+                                                  uint32_t mask0, uint32_t* bm, uint32_t lane) {
   for (uint32_t i = lane; i < wn; i += 32) {
     const uint2 w = pw[i];
-    if (KIND == kPivotBitmap || w.x >= base_w) bm[w.x - base_w] = w.y;
+    if (KIND == kPivotBitmap || w.x >= base_w) bm[w.x - base_w] = i == 0 ? (w.y & mask0) : w.y;
   }
 }
 
@@ -809,7 +884,7 @@ __device__ __noinline__ uint32_t fused_wide(volatile FusedFrame* fr, uint32_t ki
   if (kind == kPivotSplit) {
     const uint32_t rlen = fr->rlen;
     for (uint32_t i = lane; i < rlen; i += 32) res[i] = prow[i];
-    fused_build_words<kPivotSplit>((const uint2*)fr->gw + fr->ws, fr->wn, fr->base >> 5, bm, lane);
+    fused_build_words<kPivotSplit>((const uint2*)fr->gw + fr->ws, fr->wn, fr->base >> 5, fr->mask0, bm, lane);
     __syncwarp();
     return fused_probe<kPivotSplit>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
   }
@@ -871,17 +946,24 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
       {
         const uint32_t b = fr->b;
         const uint32_t ee = min(fr->rp[b + 1], fr->e1);
-        const uint32_t v = fr->pivot_base + b;
-        const uint32_t ps = fr->gp[v];
-        const uint32_t pd = fr->gp[v + 1] - ps;
-        const uint32_t ws = fr->wp[v];
-        const uint32_t wn = fr->wp[v + 1] - ws;
-        fused_choose(fr, fr->gi + ps, pd, bm_words, lane);
+        const uint32_t lo = fr->pivot_base;
+        const uint32_t v = lo + b;
+        const uint32_t* gi = fr->gi;
+        uint32_t ps = fr->gp[v];
+        uint32_t pd = fr->gp[v + 1] - ps;
+        uint32_t ws = fr->wp[v];
+        uint32_t wn = fr->wp[v + 1] - ws;
+        uint32_t mask0 = FULL;
+        // ids of N+(v) below the task columns (never, for a CSR oriented from
+        // lower to higher ids) are left out of the pivot
+        if (pd > 0 && gi[ps] < lo) pivot_suffix(gi, (const uint2*)fr->gw, lo, ps, pd, ws, wn, mask0);
+        fused_choose(fr, gi + ps, pd, bm_words, lane);
         if (lane == 0) {
           fr->ee = ee;
           fr->ps = ps;
           fr->ws = ws;
           fr->wn = wn;
+          fr->mask0 = mask0;
         }
         __syncwarp();
       }
@@ -892,7 +974,8 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
         uint32_t* res = bm + fr->words + 1;
         switch (kind) {
           case kPivotBitmap:
-            fused_build_words<kPivotBitmap>((const uint2*)fr->gw + fr->ws, fr->wn, fr->base >> 5, bm, lane);
+            fused_build_words<kPivotBitmap>((const uint2*)fr->gw + fr->ws, fr->wn, fr->base >> 5, fr->mask0, bm,
+                                            lane);
             __syncwarp();
             acc += fused_probe<kPivotBitmap>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
             break;
@@ -1111,25 +1194,33 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
     for (uint32_t t = 0; t < ntasks; t++) {
       const uint32_t units = plan->prefix[t + 1] - plan->prefix[t];
       const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>((units + wpb - 1) / wpb, ctx->sms * 8));
-      k_count_task<<<grid, wpb * 32, sm, s>>>(plan->d_tasks + t, units, outs, bmw, ctx->d_unit_counter + 1);
+      k_count_task<<<grid, wpb * 32, sm, s>>>(plan->d_tasks + t, units, outs, bmw, ctx->d_unit_counter + 1,
+                                              ctx->debug_stage_polls);
       BBTC_CUDA(cudaGetLastError());
       plan->launches++;
     }
   } else {
     // the register budget: 4, 6 (default) or 8 resident blocks per SM
     const uint32_t occ = o.occupancy >= 8 ? 8 : (o.occupancy >= 6 ? 6 : 4);
-    auto* kern = plan->fused ? (occ == 8 ? k_fused_queue<8> : (occ == 6 ? k_fused_queue<6> : k_fused_queue<4>))
-                             : (occ == 8 ? k_count_queue<8> : (occ == 6 ? k_count_queue<6> : k_count_queue<4>));
+    auto* fkern = occ == 8 ? k_fused_queue<8> : (occ == 6 ? k_fused_queue<6> : k_fused_queue<4>);
+    auto* qkern = occ == 8 ? k_count_queue<8> : (occ == 6 ? k_count_queue<6> : k_count_queue<4>);
     int per_sm = 0;
-    BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, sm));
+    if (plan->fused)
+      BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fkern, wpb * 32, sm));
+    else
+      BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qkern, wpb * 32, sm));
     per_sm = std::max(1, per_sm);
     if (o.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)o.blocks_per_sm);
     // no more blocks than the queue has units for a warp each (a small batch
     // leaves the rest of the GPU to other streams)
     const uint64_t want = ((uint64_t)plan->total_units + wpb - 1) / wpb;
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)ctx->sms * per_sm, want));
-    kern<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units, ctx->d_unit_counter,
-                                    outs, bmw);
+    if (plan->fused)
+      fkern<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units,
+                                       ctx->d_unit_counter, outs, bmw);
+    else
+      qkern<<<grid, wpb * 32, sm, s>>>(plan->d_tasks, plan->d_prefix, ntasks, plan->total_units,
+                                       ctx->d_unit_counter, outs, bmw, ctx->debug_stage_polls);
     BBTC_CUDA(cudaGetLastError());
     plan->launches = 1;
   }
@@ -1209,6 +1300,12 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
     }
     plan->captured = false;
   }
+  if (plan->stage_polls != ctx->debug_stage_polls && plan->exec) {  // the launches take it as an argument
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+    plan->captured = false;
+  }
+  plan->stage_polls = ctx->debug_stage_polls;
   if (!o.use_cuda_graph) return enqueue_launches(ctx, plan, o, d_outs, (uint32_t)graphs.size());
   if (!plan->captured) {
     cudaGraph_t graph = nullptr;
@@ -1308,9 +1405,13 @@ __global__ void __launch_bounds__(256, 4) k_count_csr_static(const uint32_t* __r
     const uint64_t e1w = (uint64_t)e0 + kNoAllocUnitEdges;
     const uint32_t e1 = (uint32_t)(e1w < m ? e1w : m);
     uint32_t e = e0;
-    uint32_t u = row_of(indptr, n, e);
+    uint32_t u = row_of(indptr, n, e);  // < n (the host refuses n == 0 with m > 0)
     unsigned long long acc = 0;
     while (e < e1) {
+      if (u >= n) {  // no row ends after e: indptr[n] < m
+        if (lane == 0) atomicOr(&scr->error, 1u);
+        break;
+      }
       const uint32_t a = indptr[u], b = indptr[u + 1];
       if (b < a || (uint64_t)b > m || b <= e) {  // malformed row pointers: stop this unit
         if (lane == 0) atomicOr(&scr->error, 1u);
@@ -1363,9 +1464,33 @@ __global__ void k_noalloc_total(NoAllocScratch* scr, uint32_t units) {
 
 namespace {
 
-// Device address of g_noalloc_scratch, looked up once per device.
+// Per device, set up by the first call on it: the device address of
+// g_noalloc_scratch, the kernel's shared-memory attribute and its grid.
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[kMaxDevices] = {};
+uint32_t g_noalloc_grid[kMaxDevices] = {};
+
+constexpr uint32_t kNoAllocBitmapWords = 1024, kNoAllocWarps = 8;
+
+int noalloc_setup(int dev, void** ptr, uint32_t* grid) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    // the device is current: resolve the array's device address
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    const size_t sm = smem_bytes(kNoAllocBitmapWords, kNoAllocWarps);
+    BBTC_CUDA(cudaFuncSetAttribute(k_count_csr_static, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int sms = 0, per_sm = 0;
+    BBTC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count_csr_static, kNoAllocWarps * 32, sm));
+    g_noalloc_grid[dev] = (uint32_t)std::max(1, sms * std::max(1, per_sm));
+    g_noalloc_ptr[dev] = p;
+  }
+  *ptr = g_noalloc_ptr[dev];
+  *grid = g_noalloc_grid[dev];
+  return BBTC_OK;
+}
 
 }  // namespace
 
@@ -1376,6 +1501,7 @@ extern "C" int bbtc_count_csr_noalloc(const uint32_t* d_indptr, const uint32_t* 
   using namespace bbtc;
   if (!d_indptr || (m && !d_indices) || !out) return fail(BBTC_ERR_ARG, "NULL argument");
   if (n == 0xffffffffu) return fail(BBTC_ERR_ARG, "n must be below 2^32 - 1");
+  if (n == 0 && m > 0) return fail(BBTC_ERR_ARG, "a CSR with no rows cannot hold edges (n == 0, m > 0)");
   if (m > kNoAllocMaxEdges)
     return fail(BBTC_ERR_CAPACITY, "bbtc_count_csr_noalloc takes at most " + std::to_string(kNoAllocMaxEdges) +
                                        " oriented edges (its static scratch has one slot per 256 edges); got " +
@@ -1385,31 +1511,16 @@ extern "C" int bbtc_count_csr_noalloc(const uint32_t* d_indptr, const uint32_t* 
   if (dev < 0 || dev >= (int)kMaxDevices) return fail(BBTC_ERR_NODEV, "device index beyond the supported range");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   void* ptr = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-      // first call on this device (which is current): resolve the array's device address
-      const cudaError_t e = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        g_noalloc_ptr[dev] = nullptr;
-        return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-      }
-    }
-    ptr = g_noalloc_ptr[dev];
-  }
+  uint32_t grid = 0;
+  BBTC_TRY(noalloc_setup(dev, &ptr, &grid));
   NoAllocScratch* scr = static_cast<NoAllocScratch*>(ptr);
   // head, error and total start at zero; the partials of this call's units are all rewritten
   BBTC_CUDA(cudaMemsetAsync(scr, 0, offsetof(NoAllocScratch, pad), s));
   const uint32_t units = (uint32_t)((m + kNoAllocUnitEdges - 1) / kNoAllocUnitEdges);
   if (units > 0) {
-    const uint32_t bmw = 1024, wpb = 8;
-    const size_t sm = smem_bytes(bmw, wpb);
-    BBTC_CUDA(cudaFuncSetAttribute(k_count_csr_static, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    int sms = 0, per_sm = 0;
-    BBTC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    BBTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count_csr_static, wpb * 32, sm));
-    const uint32_t grid = (uint32_t)std::max(1, sms * std::max(1, per_sm));
-    k_count_csr_static<<<grid, wpb * 32, sm, s>>>(d_indptr, d_indices, n, m, units, scr, bmw);
+    const size_t sm = smem_bytes(kNoAllocBitmapWords, kNoAllocWarps);
+    k_count_csr_static<<<grid, kNoAllocWarps * 32, sm, s>>>(d_indptr, d_indices, n, m, units, scr,
+                                                              kNoAllocBitmapWords);
     BBTC_CUDA(cudaGetLastError());
     k_noalloc_total<<<1, 1024, 0, s>>>(scr, units);
     BBTC_CUDA(cudaGetLastError());

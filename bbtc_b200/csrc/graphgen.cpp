@@ -215,19 +215,16 @@ int gen_chung_lu(uint32_t n, double gamma, double mean_deg, double max_deg, uint
   }
   const double i0 = std::sqrt(lo * hi);
   std::vector<double> w(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; i++) w[i] = std::pow((double)i + i0, -alpha);
+  // the sums run in index order: the graph must not depend on the thread count
   double sum = 0;
-#pragma omp parallel for schedule(static) reduction(+ : sum)
-  for (int64_t i = 0; i < (int64_t)n; i++) {
-    w[i] = std::pow((double)i + i0, -alpha);
-    sum += w[i];
-  }
+  for (uint32_t i = 0; i < n; i++) sum += w[i];
   const double scale = mean_deg * n / sum;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; i++) w[i] = std::min(w[i] * scale, max_deg);
   double S = 0;
-#pragma omp parallel for schedule(static) reduction(+ : S)
-  for (int64_t i = 0; i < (int64_t)n; i++) {
-    w[i] = std::min(w[i] * scale, max_deg);
-    S += w[i];
-  }
+  for (uint32_t i = 0; i < n; i++) S += w[i];
   // weights are non-increasing in i, as the skipping method requires
   const int nt = omp_get_max_threads();
   std::vector<std::vector<uint32_t>> es(nt), ed(nt);

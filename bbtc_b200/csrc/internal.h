@@ -141,6 +141,7 @@ struct Plan {
   cudaEvent_t h_done = nullptr;    // recorded after the last upload from h_buf
   cudaGraphExec_t exec = nullptr;
   bool captured = false;
+  uint32_t stage_polls = 0;        // the context's staging test hook when the launch was captured
   void release();
 };
 
@@ -157,6 +158,8 @@ struct bbtc_ctx {
   uint32_t upload_window = 0;          // host uploads: pieces in flight at most (0 = all at once)
   uint64_t zero_copy_bytes = 0;        // host arrays up to this size in mapped page-locked memory are read
                                        // by a kernel instead of the copy engines (0 = never)
+  uint32_t debug_stage_polls = 0;      // test hook (bbtc_debug_stage_timeout): > 0 = staging copies are not
+                                       // issued and their waits give up after this many polls
   // Page-locked staging for the small control copies (cut vectors, tile
   // offsets and statistics, counts).  A copy to or from pageable memory is
   // staged by the driver through buffers every thread shares, so one that

@@ -14,8 +14,10 @@
 //   * reversed tiles (y, x): the same edges grouped by their column vertex --
 //     the CSC of forward tile (x, y) -- with, beside each entry, the record
 //     of its forward edge (u, v): the range of row u's word-compressed pairs
-//     from the one that holds v to the row's end, which is what a fused task
-//     row streams per entry;
+//     from the one that holds v (or, when the pivot row N+(v) has ids below
+//     v inside the task columns, from the first pair that can hold one: see
+//     record_start) to the row's end, which is what a fused task row streams
+//     per entry;
 //   * the word-compressed rows of the oriented CSR: row u's ids grouped by
 //     32-id word into (word index, bit mask) pairs.
 //
@@ -236,14 +238,49 @@ __global__ void k_row_index(const uint32_t* __restrict__ rp, const uint64_t* __r
   }
 }
 
+// First pair of a reversed entry's record.  The entry (row v of part x,
+// column c) stands for forward edge c -> v; the tasks (i, x, k >= x) count the
+// common neighbours w of c and v with w >= cuts[x] (the reference's tiles
+// ac = (i, k), bc = (x, k), src/triangle_counting/gpu_sparse_kernel.cu:25-46).
+// The pivot side of v keeps only N+(v) ∩ [cuts[x], ∞), whose first id is L;
+// the streamed side is row c from the first pair whose word can hold an id
+// >= L.  When L lies in v's word or above -- always for a CSR oriented from
+// lower to higher ids, where every id of N+(v) exceeds v -- that is the pair
+// holding v itself (`p`); otherwise the pair is searched in row c's pairs
+// before p.  Any CSR that meets the input contract counts the reference's
+// task sum this way.
+__device__ __forceinline__ uint32_t record_start(const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fidx,
+                                                 const uint2* __restrict__ words, const uint32_t* __restrict__ wptr,
+                                                 uint32_t v, uint32_t c, uint32_t lo, uint32_t p) {
+  const uint32_t a = fptr[v], b = fptr[v + 1];
+  if (a >= b) return p;  // no pivot: the kernel skips the row
+  uint32_t L = fidx[a];
+  if (L < lo) {
+    const uint32_t k = lower_bound_range(fidx, a, b, lo);
+    if (k >= b) return p;  // no pivot id in the task columns
+    L = fidx[k];
+  }
+  const uint32_t lw = L >> 5;
+  if (lw >= (v >> 5)) return p;
+  uint32_t lo_p = wptr[c], hi_p = p;  // row c holds v, so the answer is at or before p
+  while (lo_p < hi_p) {
+    const uint32_t mid = lo_p + ((hi_p - lo_p) >> 1);
+    if (words[mid].x < lw) lo_p = mid + 1; else hi_p = mid;
+  }
+  return lo_p;
+}
+
 // Scatter tile-local column ids (and, for the reversed graph, the records of
-// the forward edges) into the column pool.
+// the forward edges) into the column pool.  For the reversed graph
+// `fptr` / `fidx` / `words` are the oriented CSR and its word-compressed rows.
 __global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
                                 const uint32_t* __restrict__ rows, uint64_t m, const uint32_t* __restrict__ cuts_g,
                                 uint32_t P, const uint64_t* __restrict__ rp_off, const uint64_t* __restrict__ col_off,
                                 const uint32_t* __restrict__ rp, uint32_t* __restrict__ col,
                                 const uint32_t* __restrict__ eids, const uint32_t* __restrict__ wpos,
-                                const uint32_t* __restrict__ wptr, uint2* __restrict__ rec) {
+                                const uint32_t* __restrict__ wptr, uint2* __restrict__ rec,
+                                const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fidx,
+                                const uint2* __restrict__ words) {
   __shared__ uint32_t cuts[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
   __syncthreads();
@@ -260,9 +297,9 @@ __global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint3
     col[pos] = c - cuts[y];
     if (rec) {
       // forward edge fe = (c -> u) of this reversed entry: the pairs of row c
-      // from the one holding u to the row's end
+      // from the record's first pair to the row's end
       const uint32_t fe = eids[e];
-      rec[pos] = make_uint2(wpos[fe], wptr[c + 1]);
+      rec[pos] = make_uint2(record_start(fptr, fidx, words, wptr, u, c, cuts[x], wpos[fe]), wptr[c + 1]);
     }
   }
 }
@@ -375,7 +412,8 @@ bool mapped_host_range(const void* p, size_t bytes) {
 int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const uint32_t* d_indices,
                 const uint32_t* d_rows, uint32_t n, uint64_t m, const std::vector<uint32_t>& cuts,
                 const uint32_t* d_cuts, const uint32_t* eids, const uint32_t* wpos, const uint32_t* wptr,
-                uint32_t* d_stats, uint64_t* d_coloff, int grid) {
+                const uint32_t* fptr, const uint32_t* fidx, const uint2* words, uint32_t* d_stats,
+                uint64_t* d_coloff, int grid) {
   const uint32_t P = (uint32_t)cuts.size() - 1;
   const uint32_t T = P * P;
   cudaStream_t s = ctx->stream;
@@ -449,7 +487,8 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   }
   if (m > 0) {
     k_entry_scatter<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
-                                         bt.d_col, eids, wpos, wptr, reinterpret_cast<uint2*>(bt.d_rec));
+                                         bt.d_col, eids, wpos, wptr, reinterpret_cast<uint2*>(bt.d_rec), fptr, fidx,
+                                         words);
     BBTC_CUDA(cudaGetLastError());
   }
   return BBTC_OK;
@@ -700,7 +739,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     // reversed entries: row = column vertex v (keys), column = source u, record of forward edge (u, v)
     BBTC_TRY(build_block(ctx, g->rev, rev_indptr.as<uint32_t>(), rev_cols.as<uint32_t>(), keys_out.as<uint32_t>(),
                          n, m, g->cuts, d_cuts.as<uint32_t>(), eids_out.as<uint32_t>(), wpos.as<uint32_t>(),
-                         g->d_wptr, stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), grid));
+                         g->d_wptr, d_indptr, d_indices, reinterpret_cast<const uint2*>(g->d_words),
+                         stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), grid));
   }
   // the host needs the tile statistics only now: one read-back for both block CSRs
   BBTC_TRY(fetch_stats(ctx, nullptr, g->rev, nullptr, nullptr, stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), s));
@@ -742,8 +782,8 @@ int build_fwd(bbtc_graph* g) {
     BBTC_CUDA(cudaGetLastError());
   }
   BBTC_TRY(build_block(ctx, g->fwd, g->d_indptr, g->d_indices, rows.as<uint32_t>(), n, m, g->cuts,
-                       d_cuts.as<uint32_t>(), nullptr, nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(),
-                       grid));
+                       d_cuts.as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                       stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
   BBTC_TRY(fetch_stats(ctx, nullptr, g->fwd, nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(), s));
   g->fwd_built = true;
   g->device_bytes += block_bytes(g->fwd, false);

@@ -21,8 +21,10 @@
 //     column part (so every edge sits in exactly one tile); the tile's longest
 //     row and non-empty row count are right; the row index of every 32nd entry
 //     names the row holding that entry;
-//   * the reversed tiles' records: entry (v, u) holds the pair of row u that
-//     contains v and the end of row u's pairs.
+//   * the reversed tiles' records: entry (v, u) of row part x holds the end of
+//     row u's pairs and its first pair: the one that contains v, or -- when
+//     the first id L of v's row at or above cuts[x] lies in a lower 32-id
+//     word than v -- the first pair of row u whose word is >= L / 32.
 // Each check returns "" or a message naming the first broken rule.
 #pragma once
 
@@ -132,6 +134,16 @@ inline bool disjoint(std::vector<std::pair<uint64_t, uint64_t>> seg) {
   return true;
 }
 
+// Word of the first id >= lo in row v of the word rows (~0u when there is none).
+inline uint32_t record_word(const Words& w, uint32_t v, uint32_t lo) {
+  for (uint32_t p = w.wptr[v]; p < w.wptr[v + 1]; p++) {
+    const uint32_t word = w.pairs[2 * p], mask = w.pairs[2 * p + 1];
+    for (uint32_t bit = 0; bit < 32; bit++)
+      if ((mask >> bit & 1) && word * 32 + bit >= lo) return word;
+  }
+  return ~0u;
+}
+
 // `src` is the CSR the block CSR splits (the oriented graph for the forward
 // tiles, its transpose for the reversed ones); `w` holds the oriented graph's
 // word rows, read only for the records.  Rows >= src.n (cuts[P] may exceed n)
@@ -196,8 +208,13 @@ inline std::string tiles(const char* name, const Csr& src, const Tiles& t, const
             const uint32_t p0 = t.rec[2 * (co + s + q)], p1 = t.rec[2 * (co + s + q) + 1];
             if (p1 != w.wptr[fu + 1] || p0 < w.wptr[fu] || p0 >= p1)
               return pre + at("record outside the row's pairs, tile / row", id, b);
-            if (w.pairs[2 * p0] != v / 32 || !(w.pairs[2 * p0 + 1] >> (v % 32) & 1))
+            const uint32_t lw = record_word(w, v, t.cuts[x]);
+            if (lw < v / 32) {
+              if (w.pairs[2 * p0] < lw || (p0 > w.wptr[fu] && w.pairs[2 * (p0 - 1)] >= lw))
+                return pre + at("record names the wrong pair, tile / row", id, b);
+            } else if (w.pairs[2 * p0] != v / 32 || !(w.pairs[2 * p0 + 1] >> (v % 32) & 1)) {
               return pre + at("record names the wrong pair, tile / row", id, b);
+            }
           }
         }
         for (uint32_t q = (s + 31) & ~31u; q < e; q += 32)

@@ -44,6 +44,54 @@ class OrientedCSR:
         s = int(d[rows].sum()) + int(d[self.indices.astype(np.int64)].sum())
         return 4 * self.m + 4 * s
 
+    def fused_bytes(self, cuts) -> dict:
+        """Bytes one count by fused task rows reads at least, each byte once
+        per use (no reuse through the caches), for a CSR oriented from lower
+        to higher ids:
+
+        * 8 per streamed (32-id word, bit mask) pair: in-edge (u, v) streams
+          the pairs of N+(u) from the one holding v to the row's end;
+        * 8 per in-edge record (first pair, end pair);
+        * per pivot visit -- vertex v once per row part i that holds one of
+          its in-neighbours (reversed tile (part(v), i)) -- its word pairs
+          (8 each) and 28 bytes of row pointers and first / last ids.
+
+        Returns the total and its parts."""
+        n, m = self.n, self.m
+        ip = self.indptr.astype(np.int64)
+        ix = self.indices
+        if m == 0:
+            return {"bytes": 0, "pairs_streamed": 0, "pivot_visits": 0, "pivot_pairs": 0, "records": 0}
+        w = ix >> 5
+        flags = np.empty(m, dtype=np.int64)
+        flags[0] = 1
+        flags[1:] = w[1:] != w[:-1]
+        starts = ip[:-1][ip[:-1] < ip[1:]]
+        flags[starts] = 1  # a row's first id opens a pair
+        cf = np.zeros(m + 1, dtype=np.int64)
+        np.cumsum(flags, out=cf[1:])
+        del flags
+        wptr = cf[ip]  # pairs before each row
+        deg = np.diff(ip)
+        # sum over edges e of (end pair of its row - pair holding e) = sum_u d(u) wptr[u+1] - sum_e (cf[e+1] - 1)
+        streamed = int((deg * wptr[1:]).sum()) - int(cf[1:].sum()) + m
+        del cf
+        cuts = np.asarray(cuts, dtype=np.int64)
+        P = len(cuts) - 1
+        part_of_row = np.searchsorted(cuts, np.arange(n, dtype=np.int64), side="right") - 1
+        seen = np.zeros((n, P), dtype=np.uint8)
+        src_part = np.repeat(part_of_row, deg)
+        seen[ix.astype(np.int64), src_part] = 1
+        del src_part
+        visits_per_v = seen.sum(axis=1, dtype=np.int64)
+        del seen
+        wn = np.diff(wptr)
+        visits = int(visits_per_v.sum())
+        pivot_pairs = int((visits_per_v * wn).sum())
+        total = 8 * streamed + 8 * m + 8 * pivot_pairs + 28 * visits
+        return {"bytes": total, "pairs_streamed": streamed, "pivot_visits": visits, "pivot_pairs": pivot_pairs,
+                "records": m}
+
 
 def _take(handle: ctypes.c_void_p, name: str, meta: dict) -> OrientedCSR:
     lib = _lib.host()

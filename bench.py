@@ -228,20 +228,38 @@ def make_graph(args, seed):
     return g, cuts, time.time() - t0
 
 
+def reference_graph(args, seed):
+    """The benchmark graph and the reference's own cut vector, from oracle/
+    code only: the generators' restatement (oracle/graphs_oracle.c, bit-equal
+    to the library's) and the reference's SARMA partitioner (oracle/_ref)."""
+    import oracle
+    t0 = time.time()
+    if args.family == "chunglu":
+        n, indptr, indices = oracle.chung_lu(1 << args.scale, 2.1, 20.0, 50000.0, seed=seed)
+    else:
+        n, indptr, indices = oracle.rmat(args.scale, args.edge_factor, seed=seed)
+    part = "pal" if args.partitioner.startswith("pal") else args.partitioner
+    cuts = oracle.ref_cuts(n, indptr, indices, args.ncut, part)
+    return n, indptr, indices, cuts, time.time() - t0
+
+
 def run_reference(args, rank: int):
-    """Reference arm: the reference's own CPU counting path, all host threads."""
+    """Reference arm: the reference's own CPU counting path on all host
+    threads, fed the same graph (generated by the oracle's restatement) and
+    cut by the reference's own SARMA partitioner; nothing of this library is
+    loaded."""
     import oracle
     if rank != 0:
         return None
     if not oracle.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libbbtc_ref.so not built"}
-    g, cuts, _ = make_graph(args, args.seed)
+    n, indptr, indices, cuts, gen_s = reference_graph(args, args.seed)
+    m = int(indices.shape[0])
     threads = args.cpu_threads or os.cpu_count()
-    count, secs = oracle.ref_count(g.n, g.indptr, g.indices, cuts, nthreads=threads,
-                                   repeat=args.warmup + args.steps)
+    count, secs = oracle.ref_count(n, indptr, indices, cuts, nthreads=threads, repeat=args.warmup + args.steps)
     timed = secs[args.warmup:]
     t = statistics.median(timed)
-    value = g.m / t
+    value = m / t
     sample = (f"full workload per step: NoOfTriangles() over all {args.ncut * (args.ncut + 1) * (args.ncut + 2) // 6}"
               f" tasks, median of {len(timed)} steps after {args.warmup} warm-up")
     return {
@@ -249,8 +267,10 @@ def run_reference(args, rank: int):
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "device": "host cores (rank 0 only)", "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"{workload_name(args)} {args.partitioner} "
-                               f"ncut {args.ncut}", "n": g.n, "m": g.m, "triangles": count},
+        "config": {"workload": f"{workload_name(args)} {args.partitioner} ncut {args.ncut}", "n": n, "m": m,
+                   "P": args.ncut, "partitioner": args.partitioner, "triangles": count,
+                   "cuts": "the reference's SARMA partitioner (include/utils/utils.hpp:271-288)",
+                   "graph": "oracle/graphs_oracle.c (the generators' restatement)", "generate_s": round(gen_s, 2)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -539,6 +559,29 @@ def main():
         pt = sum(ptimes) / len(ptimes) / 1e3
         plain = {"value": g.m / pt, "unit": UNIT, "ms_per_step": pt * 1e3,
                  "launches_per_step": plaunches // len(ptimes), "persistent_over_plain": pt / t_mean}
+        # the same per-task kernel as the plain form, every task's units in one
+        # persistent launch from the device queue: separates the queue's gain
+        # from the fused task rows' algorithmic gain
+        qo = options(mode="persistent", kernel="bitmap", bitmap_words=args.bitmap_words, cuda_graph=True)
+        tl = st.task_list(sorted=True)
+        qtimes, qcounts = [], set()
+        for i in range(2 + max(3, args.steps // 2)):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                st.count_async(tl, opts=qo)  # an explicit per-task kernel: the task queue, not task rows
+                e1.record(stream)
+            qcounts.add(st.count_wait())
+            if i >= 2:
+                qtimes.append(e0.elapsed_time(e1))
+        assert qcounts == {count}, f"per-task queue disagrees: {qcounts} vs {count}"
+        qt = sum(qtimes) / len(qtimes) / 1e3
+        plain["persistent_per_task"] = {
+            "value": g.m / qt, "unit": UNIT, "ms_per_step": qt * 1e3, "launches_per_step": 1,
+            "kernel": "per-task bitmap (k_count_queue), every task of the sorted list in one launch",
+            "over_plain": pt / qt, "fused_over_per_task": qt / t_mean}
 
     # --- e2e through the C ABI from pinned host buffers ---
     e2e = None
@@ -577,15 +620,20 @@ def main():
         import oracle
         if oracle.ref_available():
             threads = args.cpu_threads or os.cpu_count()
-            rc, secs = oracle.ref_count(g.n, g.indptr, g.indices, cuts, nthreads=threads, repeat=1)
+            part = "pal" if args.partitioner.startswith("pal") else args.partitioner
+            rcuts = oracle.ref_cuts(g.n, g.indptr, g.indices, args.ncut, part)
+            rc, secs = oracle.ref_count(g.n, g.indptr, g.indices, rcuts, nthreads=threads, repeat=1)
             ref_match = (rc == count)
             cpu = {"value": g.m / secs[0], "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": "the full workload once: the reference's NoOfTriangles() over all tasks of the "
-                             "same graph and cuts (oracle/_ref, built from the reference's sources)",
+                             "same graph, cut by the reference's own SARMA partitioner (oracle/_ref, built from "
+                             "the reference's sources)",
                    "seconds": secs[0], "count_matches_gpu": ref_match}
 
     peak, peak_kind = peaks()
-    achieved = balg / t_mean / 1e9
+    fb = g.fused_bytes(cuts) if args.kernel in ("auto", "fused") else None
+    model_bytes = fb["bytes"] if fb else balg
+    achieved = model_bytes / t_mean / 1e9
     traffic, traffic_note = load_traffic(args.family, args.scale, args.ncut)
     res = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -605,16 +653,21 @@ def main():
         "e2e": e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes": balg, "peak_note": "of measured (MEASURED_PEAKS.json hbm_gbs)"
+                     "model_bytes": model_bytes, "model": ("fused task rows" if fb else "B_alg"),
+                     "model_parts": fb,
+                     "peak_note": "of measured (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "of fallback",
+                     "algorithmic_bytes_merge": balg, "merge_frac": balg / t_mean / 1e9 / peak,
                      "dram_gbs": (traffic / t_mean / 1e9) if traffic else None,
                      "dram_frac": (traffic / t_mean / 1e9 / peak) if traffic else None,
-                     "note": ("achieved = B_alg / count time, B_alg = 4m + 4 sum over edges (u,v) of d+(u) + d+(v), "
-                              "the ids a merge intersection streams; the kernel streams 8-byte word-compressed "
-                              "pairs (one per 32-id word) against a shared-memory bitmap and hits L2 for reused "
-                              "rows, so its DRAM traffic is a few percent of B_alg and frac exceeds 1; dram_gbs "
-                              "is the ncu-measured DRAM traffic over the same time"
-                              + (f"; traffic: {traffic_note}" if traffic_note else ""))},
+                     "note": ("achieved = model bytes / count time (CUDA events on the library's stream). Model "
+                              "(fused task rows, the default path): 8 B per streamed (32-id word, bit mask) pair "
+                              "(in-edge (u, v) streams N+(u) from v's word to the row's end), 8 B per in-edge "
+                              "record, and per pivot visit its word pairs plus 28 B of row pointers and bounds -- "
+                              "each byte once per use, no cache reuse. merge_frac: the same time against B_alg = "
+                              "4m + 4 sum over edges of d+(u) + d+(v), the ids a merge intersection streams, "
+                              "which this kernel does not read. dram_gbs: ncu DRAM traffic of one launch over the "
+                              "same time" + (f"; traffic: {traffic_note}" if traffic_note else ""))},
         "cpu_baseline": cpu,
         "gpu_launches": launches,
         "clocks": clk,

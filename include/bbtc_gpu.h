@@ -59,6 +59,14 @@ int bbtc_version(void);
  * Process-wide (all contexts and threads). */
 int bbtc_debug_fail_alloc(int64_t after, int64_t* left);
 
+/* Test hook for the bounded device waits: with polls > 0, the per-task
+ * kernels of this context (BBTC_KERNEL_BITMAP / SEARCH) no longer issue their
+ * shared-memory staging copies, and each staging wait gives up after `polls`
+ * polls, as it would for a copy that never lands: the count is void and the
+ * call returns BBTC_ERR_TIMEOUT, with nothing left in flight.  0 restores
+ * normal staging.  No reference counterpart (it checks no wait or error). */
+int bbtc_debug_stage_timeout(bbtc_ctx* ctx, uint32_t polls);
+
 /* ---- context: device, stream, scratch ------------------------------------
  * Replaces BBTc's constructor GPU set-up and PrepareGpu
  * (src/triangle_counting/bb_tc.cpp:17-33, bb_tc_helper.cpp:53-73): one
@@ -328,13 +336,17 @@ int bbtc_server_stats_get(bbtc_server* s, bbtc_server_stats* st);
  * 256 edges) is a file-scope device array of about 512 KiB that every GPU
  * loading the library holds until the process exits, so m is limited to
  * 16,777,216 oriented edges (larger m: BBTC_ERR_CAPACITY, nothing launched).
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the array and it
- * keeps the last call's contents: each call clears what must start at zero,
- * and calls that overlap on the GPU (on different streams or threads) race --
- * serialise them.  Work is enqueued on `stream` (a cudaStream_t, NULL = the
- * legacy default stream) and the call waits for it.  A row pointer or id out
- * of bounds, or an unsorted row, is reported as BBTC_ERR_INPUT. */
+ * The first call on a device (with that device current) looks up the array's
+ * device address and the kernel's launch shape, once.  All calls share the
+ * array and it keeps the last call's contents: each call clears what must
+ * start at zero, and calls that overlap on the GPU (on different streams or
+ * threads) race -- serialise them.  Work is enqueued on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream) and the call is synchronous:
+ * it waits for that stream before returning, so it must not be called while
+ * the stream is being captured.  n == 0 with m > 0 is BBTC_ERR_ARG; a row
+ * pointer or id out of bounds (indptr[n] < m included), or an unsorted row,
+ * is reported as BBTC_ERR_INPUT without reading outside the caller's arrays
+ * (indptr[n+1], indices[m]). */
 int bbtc_count_csr_noalloc(const uint32_t* d_indptr, const uint32_t* d_indices, uint32_t n, uint64_t m,
                            uint64_t* out, void* stream);
 

@@ -10,6 +10,10 @@ library (bbtc_b200) never imports it.
   (oracle/ref_harness.cpp -> oracle/_ref/libbbtc_ref.so).
 * :func:`ref_cli` -- the reference's unmodified CPU executable
   (oracle/_ref/bbtc_cpu) on an edge-list file.
+* :func:`ref_cuts` -- the reference's own SARMA cut vector (oracle/_ref).
+* :func:`rmat`, :func:`chung_lu` -- the benchmark graphs from a restatement of
+  the library's generators (oracle/graphs_oracle.c), so the timed reference
+  path loads none of the library's code.
 * :func:`brute_force` -- pure-Python count over all vertex triples, tiny graphs.
 """
 from __future__ import annotations
@@ -27,9 +31,19 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _libs: dict[str, ctypes.CDLL] = {}
 
 
+def reference_dir() -> str | None:
+    """The reference's source tree: $BBTC_REFERENCE, else the checkout beside
+    this repository (``../reference``) when it holds the reference's sources."""
+    for d in (os.environ.get("BBTC_REFERENCE"), os.path.join(os.path.dirname(HERE), "..", "reference")):
+        if d and os.path.exists(os.path.join(d, "src", "bbtc.cpp")):
+            return os.path.realpath(d)
+    return None
+
+
 def build() -> None:
     """Compile the restatement and, when the reference tree is present, oracle/_ref."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    ref = reference_dir()
+    subprocess.run(["make", "-s", "-C", HERE] + ([f"REF={ref}"] if ref else []), check=True)
 
 
 def _load(rel: str) -> ctypes.CDLL:
@@ -86,6 +100,70 @@ def tile_nnz(n: int, indptr, indices, cuts) -> np.ndarray:
     rc = lib.oracle_tile_nnz(n, _p(indptr), _p(indices), _p(cuts), P, _p(out))
     if rc != 0:
         raise RuntimeError(f"oracle_tile_nnz failed ({rc})")
+    return out
+
+
+def _take_csr(lib, n: int, m: int, ip, ix) -> tuple[int, np.ndarray, np.ndarray]:
+    try:
+        indptr = np.ctypeslib.as_array(ctypes.cast(ip, ctypes.POINTER(ctypes.c_uint32)), (n + 1,)).copy()
+        indices = (np.ctypeslib.as_array(ctypes.cast(ix, ctypes.POINTER(ctypes.c_uint32)), (m,)).copy()
+                   if m else np.zeros(0, np.uint32))
+    finally:
+        lib.oracle_free(ip)
+        lib.oracle_free(ix)
+    return n, indptr, indices
+
+
+def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+         seed: int = 1) -> tuple[int, np.ndarray, np.ndarray]:
+    """R-MAT graph, cleaned and oriented (graphs_oracle.c: oracle_rmat): the
+    same graph as bbtc_b200.graphs.rmat, built by independent code.  Returns
+    (n, indptr, indices)."""
+    lib = _load("lib/liboracle.so")
+    lib.oracle_rmat.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
+                                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
+    lib.oracle_free.argtypes = [ctypes.c_void_p]
+    n, m = ctypes.c_uint32(), ctypes.c_uint64()
+    ip, ix = ctypes.c_void_p(), ctypes.c_void_p()
+    rc = lib.oracle_rmat(scale, edge_factor, a, b, c, seed, ctypes.byref(n), ctypes.byref(m), ctypes.byref(ip),
+                         ctypes.byref(ix))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rmat failed ({rc})")
+    return _take_csr(lib, n.value, m.value, ip, ix)
+
+
+def chung_lu(n: int, gamma: float = 2.1, mean_deg: float = 20.0, max_deg: float = 50000.0,
+             seed: int = 3) -> tuple[int, np.ndarray, np.ndarray]:
+    """Chung-Lu graph, cleaned and oriented (graphs_oracle.c: oracle_chung_lu):
+    the same graph as bbtc_b200.graphs.chung_lu.  Returns (n, indptr, indices)."""
+    lib = _load("lib/liboracle.so")
+    lib.oracle_chung_lu.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                    ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
+    lib.oracle_free.argtypes = [ctypes.c_void_p]
+    m = ctypes.c_uint64()
+    ip, ix = ctypes.c_void_p(), ctypes.c_void_p()
+    rc = lib.oracle_chung_lu(n, gamma, mean_deg, max_deg, seed, ctypes.byref(m), ctypes.byref(ip), ctypes.byref(ix))
+    if rc != 0:
+        raise RuntimeError(f"oracle_chung_lu failed ({rc})")
+    return _take_csr(lib, n, m.value, ip, ix)
+
+
+PARTITIONERS = {"uni": 0, "n1d": 1, "pal": 2, "rac": 3}
+
+
+def ref_cuts(n: int, indptr, indices, ncut: int, partitioner: str = "pal") -> np.ndarray:
+    """The reference's own cut vector (oracle/_ref/libbbtc_ref.so: ref_cuts),
+    computed by its SARMA call sequence; cuts[ncut] = n + 1 as the reference sets it."""
+    lib = _load("_ref/libbbtc_ref.so")
+    indptr, indices = _u32(indptr), _u32(indices)
+    out = np.zeros(ncut + 1, dtype=np.uint32)
+    lib.ref_cuts.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
+                             ctypes.c_void_p]
+    rc = lib.ref_cuts(n, _p(indptr), _p(indices), ncut, PARTITIONERS[partitioner], _p(out))
+    if rc != 0:
+        raise RuntimeError(f"ref_cuts failed ({rc})")
     return out
 
 

@@ -21,8 +21,10 @@ struct Built {
 
 static uint64_t align4(uint64_t x) { return (x + 3) & ~3ull; }
 
-// One block CSR of `src` over the cuts; with `w`, the records of the reversed tiles.
-static Built build(const Csr& src, uint32_t P, const std::vector<uint32_t>& cuts, const Words* w) {
+// One block CSR of `src` over the cuts; with `w` (and the oriented CSR `fwd`),
+// the records of the reversed tiles.
+static Built build(const Csr& src, uint32_t P, const std::vector<uint32_t>& cuts, const Words* w,
+                   const Csr* fwd = nullptr) {
   const uint32_t T = P * P;
   Built b;
   b.rp_off.assign(T, 0);
@@ -82,10 +84,19 @@ static Built build(const Csr& src, uint32_t P, const std::vector<uint32_t>& cuts
           const uint32_t c = src.indices[a0 + q];
           b.col[pos] = c - cuts[y];
           if (w) {
-            // reversed entry (v, u): the pair of row u holding v, and row u's pair end
+            // reversed entry (v, u): the pair of row u holding v -- or, when v's
+            // row has its first id >= cuts[x] in a lower word, the first pair
+            // of row u at or above that word -- and row u's pair end
             const uint32_t v = cuts[x] + i;
+            uint32_t lw = v / 32;
+            if (fwd) {
+              // first id of v's oriented row at or above cuts[x]
+              uint32_t k = fwd->indptr[v];
+              while (k < fwd->indptr[v + 1] && fwd->indices[k] < cuts[x]) k++;
+              if (k < fwd->indptr[v + 1] && fwd->indices[k] / 32 < lw) lw = fwd->indices[k] / 32;
+            }
             uint32_t p = w->wptr[c];
-            while (w->pairs[2 * p] != v / 32) p++;
+            while (w->pairs[2 * p] < lw) p++;
             b.rec[2 * pos] = p;
             b.rec[2 * pos + 1] = w->wptr[c + 1];
           }
@@ -162,7 +173,7 @@ int main(int argc, char** argv) {
   transpose(g, tp, tc);
   Csr tr{n, m, tp.data(), tc.data()};
   Built fwd = build(g, P, cuts, nullptr);
-  Built rev = build(tr, P, cuts, &w);
+  Built rev = build(tr, P, cuts, &w, &g);
 
   uint32_t t = 0, row = 0;
   auto entry = [&](Built& b, uint32_t len) -> uint64_t {

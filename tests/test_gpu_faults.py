@@ -90,3 +90,30 @@ def test_served_request_fails_alone():
             pytest.fail("a request made more than 100 device allocations")
         assert fired >= 5
         assert srv.stats().pending == 0
+
+
+@pytest.mark.parametrize("mode", ["persistent", "plain"])
+@pytest.mark.parametrize("kernel", ["bitmap", "search"])
+def test_staging_wait_runs_out(ctx, kernel, mode):
+    """The bounded wait of the per-task kernels' shared-memory staging runs
+    out (the test hook issues no copy, so the wait can only give up, with
+    nothing in flight): the count returns BBTC_ERR_TIMEOUT, and the next count
+    on the same context and graph is right, replayed CUDA graph included."""
+    g = graphs.rmat(14, 16, seed=1)
+    cuts = graphs.cuts(g, 2, "uni")  # long tile rows: many pivots of >= 64 ids are staged
+    want = oracle.count(g.n, g.indptr, g.indices, cuts)
+    st = Graph.from_csr(ctx, g, cuts)
+    o = options(kernel=kernel, mode=mode, cuda_graph=(mode == "persistent"))
+    try:
+        assert st.count(opts=o) == want
+        ctx.debug_stage_timeout(4)
+        try:
+            with pytest.raises(BBTcError) as e:
+                st.count(opts=o)
+            assert e.value.status == -5, e.value.message
+        finally:
+            ctx.debug_stage_timeout(0)
+        for _ in range(2):
+            assert st.count(opts=o) == want
+    finally:
+        st.free()

@@ -406,3 +406,62 @@ def test_bulk_staged_pivots(ctx, kernel, mode):
         assert longest >= 64, longest
         want = oracle.count(g.n, g.indptr, g.indices, cuts)
         assert gpu_count(ctx, g, cuts, kernel=kernel, mode=mode, cuda_graph=False) == want, P
+
+
+def csr_rows(n, rows):
+    """A CSR from explicit sorted rows {row: [ids]} (any ids below n)."""
+    idx, indptr = [], np.zeros(n + 1, np.uint32)
+    for u in range(n):
+        idx += list(rows.get(u, []))
+        indptr[u + 1] = len(idx)
+    return graphs.OrientedCSR(n, indptr, np.array(idx, np.uint32))
+
+
+def random_sorted_csr(n, max_deg, seed):
+    """Rows of random distinct ids below n in increasing order: ids below the
+    row and self loops included (a CSR the input contract accepts that is not
+    an oriented graph)."""
+    rng = np.random.default_rng(seed)
+    rows = [np.unique(rng.integers(0, n, size=int(d))) for d in rng.integers(0, max_deg + 1, size=n)]
+    indptr = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint32)
+    return graphs.OrientedCSR(n, indptr, np.concatenate(rows).astype(np.uint32))
+
+
+def test_unoriented_csr_counts_the_reference_task_sum(ctx):
+    """A CSR whose rows hold ids below the row: the count is the reference's
+    task sum (its tiles keep only common neighbours in column parts k >= j),
+    on every kernel and mode, and equals the reference's own code."""
+    cases = []
+    ce = csr_rows(51, {40: [0, 50], 50: [0]})  # the reference counts 1 with P = 1
+    for cuts in ([0, 51], [0, 20, 51], [0, 40, 45, 51], [0, 33, 51], [0, 41, 52]):
+        cases.append((ce, np.array(cuts, np.uint32)))
+    for seed, (n, deg) in enumerate([(200, 30), (1000, 60), (3000, 200)]):
+        h = random_sorted_csr(n, deg, seed)
+        for P, part in ((1, "uni"), (4, "uni"), (7, "n1d")):
+            cases.append((h, graphs.cuts(h, P, part)))
+    for g, cuts in cases:
+        want = oracle.count(g.n, g.indptr, g.indices, cuts)
+        if oracle.ref_available():
+            assert oracle.ref_count(g.n, g.indptr, g.indices, cuts)[0] == want
+        for kernel, mode in KERNEL_MODES:
+            assert gpu_count(ctx, g, cuts, kernel=kernel, mode=mode) == want, (g.n, list(cuts), kernel, mode)
+    assert oracle.count(ce.n, ce.indptr, ce.indices, np.array([0, 51], np.uint32)) == 1
+
+
+@pytest.mark.parametrize("bitmap_words", [0, 64, 256])
+def test_unoriented_wide_pivots(ctx, bitmap_words):
+    """Non-oriented rows spread over a wide id range, so the fused pivots run
+    as bitmap, split, list and global-memory kinds with ids below the task
+    columns dropped."""
+    h = random_sorted_csr(1 << 15, 120, seed=9)
+    for P, part in ((3, "uni"), (8, "n1d")):
+        cuts = graphs.cuts(h, P, part)
+        want = oracle.count(h.n, h.indptr, h.indices, cuts)
+        st = Graph.from_csr(ctx, h, cuts)
+        try:
+            st.validate()
+            for kernel, mode in (("auto", "persistent"), ("fused", "plain"), ("bitmap", "persistent")):
+                got = st.count(opts=options(kernel=kernel, mode=mode, bitmap_words=bitmap_words))
+                assert got == want, (P, kernel, mode, bitmap_words)
+        finally:
+            st.free()

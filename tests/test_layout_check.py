@@ -95,3 +95,23 @@ def test_planted_faults_are_named(harness, fault):
     path = graph_file(d, g, graphs.cuts(g, 4, "pal"), "f.bin")
     out = run(exe, path, fault)
     assert out != "OK" and FAULTS[fault] in out, (fault, out)
+
+
+def random_sorted_csr(n, max_deg, seed):
+    """Rows of random distinct ids below n in increasing order: ids below the
+    row and self loops included (not an oriented graph)."""
+    rng = np.random.default_rng(seed)
+    rows = [np.unique(rng.integers(0, n, size=int(d))) for d in rng.integers(0, max_deg + 1, size=n)]
+    indptr = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint32)
+    return graphs.OrientedCSR(n, indptr, np.concatenate(rows).astype(np.uint32))
+
+
+@pytest.mark.parametrize("P,part", [(1, "uni"), (3, "uni"), (6, "n1d")])
+def test_unoriented_layout_passes(harness, P, part):
+    """A CSR whose rows hold ids below the row: the reversed tiles' records
+    start at the first pair that can meet the pivot's ids in the task columns."""
+    exe, d = harness
+    h = random_sorted_csr(300, 40, seed=P)
+    assert run(exe, graph_file(d, h, graphs.cuts(h, P, part), f"u{P}.bin"), "none") == "OK"
+    out = run(exe, graph_file(d, h, graphs.cuts(h, P, part), f"uf{P}.bin"), "rec_pair")
+    assert out != "OK" and "record" in out

@@ -114,3 +114,75 @@ def test_plants_are_caught():
     keep[ip[r + 1] - 1] = False
     ip[r + 1:] -= 1
     assert oracle.count(g.n, ip.astype(np.uint32), bad[keep], cuts) != good
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(8, 8, 1), (12, 16, 5), (16, 16, 1), (14, 32, 9)])
+def test_generator_restatement_equals_library(scale, ef, seed):
+    """The oracle's own generators (oracle/graphs_oracle.c: a global key sort
+    instead of the library's per-row buckets) give the library's graphs bit
+    for bit, so the reference arm can build them without the library."""
+    n, ip, ix = oracle.rmat(scale, ef, seed=seed)
+    g = graphs.rmat(scale, ef, seed=seed)
+    assert n == g.n and np.array_equal(ip, g.indptr) and np.array_equal(ix, g.indices)
+
+
+@pytest.mark.parametrize("n,max_deg", [(1 << 12, 500.0), (30000, 3000.0)])
+def test_chung_lu_restatement_equals_library(n, max_deg):
+    _, ip, ix = oracle.chung_lu(n, seed=3, max_deg=max_deg)
+    g = graphs.chung_lu(n, seed=3, max_deg=max_deg)
+    assert np.array_equal(ip, g.indptr) and np.array_equal(ix, g.indices)
+
+
+def random_sorted_csr(n, max_deg, seed):
+    rng = np.random.default_rng(seed)
+    rows = [np.unique(rng.integers(0, n, size=int(d))) for d in rng.integers(0, max_deg + 1, size=n)]
+    indptr = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint32)
+    return indptr, np.concatenate(rows).astype(np.uint32)
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_restatement_equals_reference_unoriented(seed):
+    """CSRs the input contract accepts that are not oriented graphs (ids
+    below the row, self loops): the restatement still gives the reference's
+    task sum, which then is not a triangle count."""
+    n = 150 * seed
+    ip, ix = random_sorted_csr(n, 25, seed)
+    rng = np.random.default_rng(seed)
+    for P in (1, 2, 5):
+        cuts = np.unique(np.concatenate([[0], rng.integers(0, n, size=P - 1), [n]])).astype(np.uint32)
+        assert oracle.count(n, ip, ix, cuts) == oracle.ref_count(n, ip, ix, cuts)[0]
+    rows = {40: [0, 50], 50: [0]}
+    ip2 = np.zeros(52, np.uint32)
+    for u in range(51):
+        ip2[u + 1] = ip2[u] + len(rows.get(u, []))
+    ix2 = np.array(rows[40] + rows[50], np.uint32)
+    assert oracle.count(51, ip2, ix2, np.array([0, 51], np.uint32)) == 1 == \
+        oracle.ref_count(51, ip2, ix2, np.array([0, 51], np.uint32))[0]
+
+
+def _row_bottleneck(g, cuts):
+    ip = g.indptr.astype(np.int64)
+    return int(np.diff(ip[np.minimum(cuts.astype(np.int64), g.n)]).max())
+
+
+@needs_ref
+@pytest.mark.parametrize("make", [lambda: graphs.rmat(14, 16, seed=2), lambda: graphs.rgg(1 << 14, seed=5),
+                                  lambda: graphs.chung_lu(1 << 15, seed=3, max_deg=3000.0)])
+@pytest.mark.parametrize("P", [4, 8, 16])
+def test_partitioners_against_sarma(make, P):
+    """The library's partitioners against the reference's own (SARMA, run by
+    the reference's call sequence in oracle/_ref): uni gives SARMA's cuts (the
+    last is n, where SARMA puts n + 1); n1d is the optimal contiguous split of
+    the row loads, so its bottleneck is at most SARMA's; pal is an
+    independent probe-a-load implementation with its own sample, so its
+    largest tile is compared, not its cuts (within 15 %)."""
+    g = make()
+    uni, ref_uni = graphs.cuts(g, P, "uni"), oracle.ref_cuts(g.n, g.indptr, g.indices, P, "uni")
+    assert np.array_equal(uni[:-1], ref_uni[:-1]) and uni[-1] == g.n and ref_uni[-1] == g.n + 1
+    n1d, ref_n1d = graphs.cuts(g, P, "n1d"), oracle.ref_cuts(g.n, g.indptr, g.indices, P, "n1d")
+    assert _row_bottleneck(g, n1d) <= _row_bottleneck(g, ref_n1d)
+    pal, ref_pal = graphs.cuts(g, P, "pal"), oracle.ref_cuts(g.n, g.indptr, g.indices, P, "pal")
+    ours = int(oracle.tile_nnz(g.n, g.indptr, g.indices, pal).max())
+    theirs = int(oracle.tile_nnz(g.n, g.indptr, g.indices, ref_pal).max())
+    assert ours <= 1.15 * theirs, (ours, theirs)
