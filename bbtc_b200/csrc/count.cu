@@ -188,6 +188,17 @@ __device__ __forceinline__ uint32_t member_word(const uint32_t* bm, const PivotV
   if constexpr (KIND == kPivotBitmap) {
     const uint32_t yw = min(w.x - (pv.base >> 5), pv.cap >> 5);
     return __popc(w.y & bm[yw]);
+  } else if constexpr (KIND == kPivotRank) {
+    // pv.base: the pivot's first word; pv.cap: its span in words; bm: one
+    // (presence bits, index of the block's first pair) entry per 32 words;
+    // pv.res: the pivot's masks in pair order.  A word the pivot lacks costs
+    // one 8-byte load.
+    const uint32_t rel = w.x - pv.base;  // words below the first wrap high
+    if (rel >= pv.cap) return 0;
+    const uint2 e = reinterpret_cast<const uint2*>(bm)[rel >> 5];
+    const uint32_t bit = 1u << (rel & 31);
+    if (!(e.x & bit)) return 0;
+    return __popc(w.y & pv.res[e.y + __popc(e.x & (bit - 1u))]);
   } else {
     if constexpr (KIND == kPivotSplit) {
       if (w.x >= (pv.base >> 5)) return __popc(w.y & bm[min(w.x - (pv.base >> 5), pv.cap >> 5)]);
@@ -747,7 +758,7 @@ enum : uint32_t { kNoPivot = 0xffffffffu };
 
 // Choose the pivot structure of row v (ids prow[0..pd)) and record it in the frame.
 __device__ __forceinline__ void fused_choose(volatile FusedFrame* fr, const uint32_t* __restrict__ prow, uint32_t pd,
-                                             uint32_t bm_words, uint32_t lane) {
+                                             uint32_t wn, uint32_t bm_words, uint32_t lane) {
   uint32_t kind = kNoPivot, base = 0, words = 0, rlen = 0;
   if (pd > 0) {
     const uint32_t first = prow[0];
@@ -758,6 +769,17 @@ __device__ __forceinline__ void fused_choose(volatile FusedFrame* fr, const uint
       base = first & ~31u;  // word-aligned: a streamed pair meets exactly one bitmap word
       words = span_words;
     } else {
+      // a wide row: a rank bitmap when its block entries (2 words per 32
+      // words of span) and masks (1 per pair) fit the buffer
+      const uint32_t blocks = (span_words + 31) >> 5;
+      if (2 * blocks + wn <= bm_words) {
+        kind = kPivotRank;
+        base = first >> 5;  // first word
+        words = blocks;
+        rlen = span_words;
+      }
+    }
+    if (kind == kNoPivot && span_words >= bm_words) {
       // bitmap over the top words of the row, the few ids below them in a short list
       const uint32_t wwords = bm_words - 1 - kSplitList;
       const uint32_t wbase = ((last >> 5) - (wwords - 1)) << 5;
@@ -817,6 +839,35 @@ __device__ __forceinline__ void fused_build_words(const uint2* __restrict__ pw, 
   }
 }
 
+// Rank pivot from its word pairs (first word fw, `blocks` entries of 32
+// words): pair i sets its presence bit, and the first pair of each block
+// writes its own index as the block's base; masks land in pair order (a
+// row's words strictly increase, so a word's rank is its pair index).
+__device__ __forceinline__ void fused_build_rank(const uint2* __restrict__ pw, uint32_t wn, uint32_t mask0,
+                                                 uint32_t fw, uint32_t blocks, uint32_t* bm, uint32_t lane) {
+  uint32_t* masks = bm + 2 * blocks;
+  for (uint32_t i = lane; i < wn; i += 32) {
+    const uint2 w = pw[i];
+    const uint32_t rel = w.x - fw;
+    const uint32_t blk = rel >> 5;
+    atomicOr(&bm[2 * blk], 1u << (rel & 31));
+    if (i == 0 || ((pw[i - 1].x - fw) >> 5) != blk) bm[2 * blk + 1] = i;
+    masks[i] = i == 0 ? (w.y & mask0) : w.y;
+  }
+}
+
+// Back to zero: the entries of the blocks that hold a pair, and the masks.
+__device__ __forceinline__ void fused_clear_rank(const uint2* __restrict__ pw, uint32_t wn, uint32_t fw,
+                                                 uint32_t blocks, uint32_t* bm, uint32_t lane) {
+  uint32_t* masks = bm + 2 * blocks;
+  for (uint32_t i = lane; i < wn; i += 32) {
+    const uint32_t blk = (pw[i].x - fw) >> 5;
+    bm[2 * blk] = 0;
+    bm[2 * blk + 1] = 0;
+    masks[i] = 0;
+  }
+}
+
 template <uint32_t KIND>
 __device__ __forceinline__ void fused_clear_words(const uint2* __restrict__ pw, uint32_t wn, uint32_t base_w,
                                                   uint32_t words, uint32_t* bm, uint32_t lane) {
@@ -865,10 +916,10 @@ __device__ __forceinline__ uint32_t fused_probe(volatile FusedFrame* fr, const u
   pv.row = prow;
   pv.len = fr->pd;
   pv.base = fr->base;
-  pv.cap = fr->words * 32;
-  pv.first = KIND == kPivotBitmap ? 0u : prow[0];
-  pv.last = KIND == kPivotBitmap ? 0u : prow[pv.len - 1];
-  pv.res = bm + fr->words + 1;
+  pv.cap = KIND == kPivotRank ? fr->rlen : fr->words * 32;
+  pv.first = KIND == kPivotBitmap || KIND == kPivotRank ? 0u : prow[0];
+  pv.last = KIND == kPivotBitmap || KIND == kPivotRank ? 0u : prow[pv.len - 1];
+  pv.res = KIND == kPivotRank ? bm + 2 * fr->words : bm + fr->words + 1;
   pv.rlen = fr->rlen;
   const RecSegs segs{(const uint2*)fr->rec};
   return probe_entries<KIND, true>(segs, e, ee, reinterpret_cast<const uint32_t*>(fr->gw), bm, sstart, sbase, pv,
@@ -957,7 +1008,7 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
         // ids of N+(v) below the task columns (never, for a CSR oriented from
         // lower to higher ids) are left out of the pivot
         if (pd > 0 && gi[ps] < lo) pivot_suffix(gi, (const uint2*)fr->gw, lo, ps, pd, ws, wn, mask0);
-        fused_choose(fr, gi + ps, pd, bm_words, lane);
+        fused_choose(fr, gi + ps, pd, wn, bm_words, lane);
         if (lane == 0) {
           fr->ee = ee;
           fr->ps = ps;
@@ -979,6 +1030,11 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
             __syncwarp();
             acc += fused_probe<kPivotBitmap>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
             break;
+          case kPivotRank:
+            fused_build_rank((const uint2*)fr->gw + fr->ws, fr->wn, fr->mask0, fr->base, fr->words, bm, lane);
+            __syncwarp();
+            acc += fused_probe<kPivotRank>(fr, prow, e, ee, bm, sstart, sbase, bm_words, lane);
+            break;
           default:
             acc += fused_wide(fr, kind, prow, e, ee, bm, sstart, sbase, bm_words, lane);
         }
@@ -990,6 +1046,7 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
           const uint2* pw = (const uint2*)fr->gw + fr->ws;
           switch (fr->kind) {
             case kPivotBitmap: fused_clear_words<kPivotBitmap>(pw, fr->wn, fr->base >> 5, fr->words, bm, lane); break;
+            case kPivotRank: fused_clear_rank(pw, fr->wn, fr->base, fr->words, bm, lane); break;
             case kPivotSplit: {
               fused_clear_words<kPivotSplit>(pw, fr->wn, fr->base >> 5, fr->words, bm, lane);
               const uint32_t rlen = fr->rlen;

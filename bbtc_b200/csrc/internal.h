@@ -89,6 +89,8 @@ enum TaskKind : uint32_t {
   kPivotGlobal = 2,  // pivot row too long for shared memory: binary search in global memory
   kFusedRow = 3,     // task row (i, j): all tasks (i, j, k >= j) in one pass, structure chosen per pivot
   kPivotSplit = 4,   // pivot row -> bitmap of its top id window + short sorted list of the ids below it
+  kPivotRank = 5,    // fused task rows: per 32-word block of the row's span a (presence bits, first pair)
+                     // entry, then the row's masks in pair order (a rank bitmap over the words)
 };
 
 // One queued task: `rows` is the tile whose rows are the pivot vertices and

@@ -45,6 +45,9 @@ sys.path.insert(0, ROOT)
 METRIC = "edges/sec at exact count, batched vs plain form on 1 B200; p50/p99 latency"
 UNIT = "edges/s"
 FALLBACK_HBM_GBS = 6650.0
+# serving throughput peak on one B200 (requests/s at which edges/s stopped
+# growing in a rate sweep); the default line serves at 80 % of it
+SERVE_PEAK_RPS = 1000.0
 
 
 def parse():
@@ -75,6 +78,8 @@ def parse():
                    help="single: one R-MAT s22 graph (default); batch: 512 R-MAT + 64 RGG graphs in one "
                         "launch; serve: Poisson request stream through the continuous-batching server")
     p.add_argument("--batch-max-scale", type=int, default=20)
+    p.add_argument("--batch-plain-steps", type=int, default=-1,
+                   help="batch: steps of the one-launch-per-task comparison (-1: steps / 2, at least 2)")
     p.add_argument("--rate", type=float, default=600.0, help="serve: requests per second")
     p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     p.add_argument("--serve-max-scale", type=int, default=22)
@@ -83,6 +88,15 @@ def parse():
     p.add_argument("--copy-engine-uploads", action="store_true",
                    help="serve: small requests go through the copy engines even from page-locked buffers")
     p.add_argument("--trace", default="", help="serve: write every request's stage timestamps to this JSON file")
+    p.add_argument("--rates", default="", help="serve: comma-separated rates, one stream each on one server")
+    p.add_argument("--no-check", action="store_true", help="batch / serve: skip the oracle counts")
+    p.add_argument("--no-batch", action="store_true", help="default line: no batched-launch sub-record")
+    p.add_argument("--no-serve", action="store_true", help="default line: no serving sub-record")
+    p.add_argument("--sub-batch-max-scale", type=int, default=14,
+                   help="default line: largest R-MAT scale of the batched-launch sub-record")
+    p.add_argument("--sub-serve-rate", type=float, default=0.0,
+                   help="default line: serving rate (0: 80 %% of SERVE_PEAK_RPS)")
+    p.add_argument("--sub-serve-duration", type=float, default=10.0)
     return p.parse_args()
 
 
@@ -297,101 +311,126 @@ def batch_workload(max_scale: int):
     return [(g, graphs.cuts(g, P, "uni")) for g, P in out]
 
 
-def run_batch(args):
+def oracle_counts(items, threads: int = 0):
+    """The oracle's count of every (graph, cuts) pair (the C restatement of
+    the reference's CPU path), largest graphs first."""
+    import oracle
+    order = sorted(range(len(items)), key=lambda i: -items[i][0].m)
+    out = [None] * len(items)
+    for i in order:
+        g, c = items[i]
+        out[i] = oracle.count(g.n, g.indptr, g.indices, c, nthreads=threads)
+    return out
+
+
+def measure_batch(ctx, max_scale: int, steps: int, warmup: int, plain_steps: int, check: bool = True) -> dict:
+    """The batched launch: every graph of the batch workload in one persistent
+    launch (bbtc_count_batch), against each graph counted alone with one
+    launch per task.  With `check`, every graph's count is first compared
+    with the oracle's."""
     import torch
-    from bbtc_b200 import Context, Graph, count_batch, options
+    from bbtc_b200 import Graph, count_batch, options
     t0 = time.time()
-    work = batch_workload(args.batch_max_scale)
+    work = batch_workload(max_scale)
     gen_s = time.time() - t0
-    ctx = Context(0)
+    t0 = time.time()
+    want = oracle_counts(work) if check else None
+    oracle_s = time.time() - t0
     sts = [Graph.from_csr(ctx, g, c) for g, c in work]
-    m_total = sum(g.m for g, _ in work)
-    alone = [st.count() for st in sts]
-    po = options(mode="persistent")
-    for _ in range(args.warmup):
-        assert count_batch(ctx, sts, po) == alone
-    ts = []
-    for _ in range(args.steps):
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        got = count_batch(ctx, sts, po)
-        ts.append(time.perf_counter() - t)
-        assert got == alone
-    plain = options(mode="plain", cuda_graph=False)
-    pts = []
-    for _ in range(max(2, args.steps // 2)):
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        got = [st.count(opts=plain) for st in sts]
-        pts.append(time.perf_counter() - t)
-        assert got == alone
-    tb, tp = statistics.median(ts), statistics.median(pts)
-    res = {"metric": METRIC, "value": m_total / tb, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": tb * 1e3, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-           "config": {"workload": f"batch: 512 R-MAT s10-{args.batch_max_scale} ef 8-32 + 64 RGG 2^14-2^18, "
-                                  f"seeds 100-675, uni ncut 4-16", "graphs": len(work), "m_total": m_total,
-                      "triangles_total": int(sum(alone)), "generate_s": round(gen_s, 1),
-                      "timing": "wall clock of bbtc_count_batch (plan + one persistent launch + readback)"},
-           "plain": {"value": m_total / tp, "ms_per_step": tp * 1e3,
-                     "note": "every graph counted alone, one launch per task",
-                     "batched_over_plain": tp / tb}}
-    print(json.dumps(res), flush=True)
-    for st in sts:
-        st.free()
+    try:
+        m_total = sum(g.m for g, _ in work)
+        po = options(mode="persistent")
+        first = count_batch(ctx, sts, po)
+        if check:
+            bad = [i for i, (a, b) in enumerate(zip(first, want)) if a != b]
+            assert not bad, f"batch counts differ from the oracle for graphs {bad[:8]}"
+        for _ in range(warmup):
+            assert count_batch(ctx, sts, po) == first
+        ts = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            got = count_batch(ctx, sts, po)
+            ts.append(time.perf_counter() - t)
+            assert got == first
+        plain = options(mode="plain", cuda_graph=False)
+        pts = []
+        for _ in range(plain_steps):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            got = [st.count(opts=plain) for st in sts]
+            pts.append(time.perf_counter() - t)
+            assert got == first
+    finally:
+        for st in sts:
+            st.free()
+    tb = statistics.median(ts)
+    res = {"value": m_total / tb, "unit": UNIT, "ms_per_step": tb * 1e3, "steps": steps,
+           "workload": f"512 R-MAT s10-{max_scale} ef 8-32 + 64 RGG 2^14-2^18, seeds 100-675, uni ncut 4-16",
+           "graphs": len(work), "m_total": m_total, "triangles_total": int(sum(first)),
+           "oracle_checked": bool(check), "generate_s": round(gen_s, 1), "oracle_s": round(oracle_s, 1),
+           "timing": "wall clock of bbtc_count_batch (plan + one persistent launch + readback)"}
+    if pts:
+        tp = statistics.median(pts)
+        res["plain"] = {"value": m_total / tp, "ms_per_step": tp * 1e3,
+                        "note": "every graph counted alone, one launch per task", "batched_over_plain": tp / tb}
+    return res
+
+
+def run_batch(args):
+    from bbtc_b200 import Context
+    ctx = Context(0)
+    plain_steps = args.batch_plain_steps if args.batch_plain_steps >= 0 else max(2, args.steps // 2)
+    b = measure_batch(ctx, args.batch_max_scale, args.steps, args.warmup, plain_steps, check=not args.no_check)
     ctx.close()
+    res = {"metric": METRIC, "value": b.pop("value"), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": b.pop("ms_per_step"), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+           "config": {"workload": "batch: " + b.pop("workload"), **{k: v for k, v in b.items() if k != "plain"}},
+           "plain": b.get("plain")}
+    print(json.dumps(res), flush=True)
 
 
-def serve_pool(max_scale: int):
+def serve_pool(max_scale: int, pin: bool):
     """Request graphs: R-MAT scale 12 + Geom(0.3) truncated at max_scale, edge
-    factor 16; a pool of distinct seeds per scale (fewer for the big ones)."""
+    factor 16; a pool of distinct seeds per scale (fewer for the big ones).
+    With `pin`, the CSRs sit in page-locked host memory, as a serving front
+    end that receives requests into pinned buffers holds them."""
+    import types
     from bbtc_b200 import graphs
+    keep = []
+
+    def pinned(a):
+        import torch
+        t = torch.empty(max(1, a.size), dtype=torch.int32, pin_memory=True)
+        t.numpy()[:a.size] = a.view(np.int32)
+        keep.append(t)
+        return t.numpy()[:a.size].view(np.uint32)
+
     pool = {}
     for s in range(12, max_scale + 1):
         k = 8 if s <= 16 else (4 if s <= 19 else 2)
         gs = []
         for j in range(k):
             g = graphs.rmat(s, 16, seed=10000 + 100 * s + j)
-            gs.append((g, graphs.cuts(g, 4 if s < 16 else 8, "pal")))
+            c = graphs.cuts(g, 4 if s < 16 else 8, "pal")
+            if pin:
+                g = types.SimpleNamespace(n=g.n, m=g.m, indptr=pinned(g.indptr), indices=pinned(g.indices))
+            gs.append((g, c))
         pool[s] = gs
-    return pool
+    return pool, keep
 
 
-def run_serve(args):
+def serve_once(srv, pool, max_scale: int, rate: float, duration: float, seed: int, want=None, trace=None) -> dict:
+    """One Poisson request stream through the server: `rate` requests/s for
+    `duration` s; latency is bbtc_submit -> count in host memory.  `want`
+    maps (scale, index) to the oracle's count of that pool graph."""
     import threading
-    from bbtc_b200 import Server
-    t0 = time.time()
-    pool = serve_pool(args.serve_max_scale)
-    gen_s = time.time() - t0
-    rng = np.random.default_rng(7)
-    n_req = max(1, int(args.rate * args.duration))
-    gaps = rng.exponential(1.0 / args.rate, size=n_req)
-    arrivals = np.cumsum(gaps)
-    scales = np.minimum(12 + rng.geometric(0.3, size=n_req) - 1, args.serve_max_scale)
-    pinned = []
-    if args.pin:
-        # request buffers in page-locked memory, as a serving front end that
-        # receives requests into pinned buffers holds them (copied into
-        # pinned allocations: registering numpy arrays fails for arrays that
-        # share a page with one already registered)
-        import types
-        import torch
-
-        def pin(a):
-            t = torch.empty(max(1, a.size), dtype=torch.int32, pin_memory=True)
-            t.numpy()[:a.size] = a.view(np.int32)
-            pinned.append(t)
-            return t.numpy()[:a.size].view(np.uint32)
-
-        for s in pool:
-            pool[s] = [(types.SimpleNamespace(n=g.n, m=g.m, indptr=pin(g.indptr), indices=pin(g.indices)), c)
-                       for g, c in pool[s]]
-    picks = [pool[int(s)][int(rng.integers(len(pool[int(s)])))] for s in scales]
-    srv = Server(0, loaders=args.loaders, copy_engine_uploads=args.copy_engine_uploads)
-    # warm-up: one request per scale
-    for s in sorted(pool):
-        g, c = pool[s][0]
-        srv.wait(srv.submit_csr(g, c))
+    rng = np.random.default_rng(seed)
+    n_req = max(1, int(rate * duration))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    scales = np.minimum(12 + rng.geometric(0.3, size=n_req) - 1, max_scale)
+    which = [int(rng.integers(len(pool[int(s)]))) for s in scales]
     ids = [None] * n_req
     start = time.perf_counter()
 
@@ -400,7 +439,7 @@ def run_serve(args):
             delay = arrivals[i] - (time.perf_counter() - start)
             if delay > 0:
                 time.sleep(delay)
-            g, c = picks[i]
+            g, c = pool[int(scales[i])][which[i]]
             ids[i] = srv.submit_csr(g, c)
 
     th = threading.Thread(target=submitter)
@@ -408,12 +447,16 @@ def run_serve(args):
     lat, lat18, edges, first_sub, last_done = [], [], 0, None, 0
     stages = {"queue": [], "load": [], "ready_wait": [], "count": []}
     by_scale = {}
-    trace = []
+    checked = 0
     for i in range(n_req):
         while ids[i] is None:
             time.sleep(0.0002)
         info = srv.wait(ids[i])
-        assert info.status == 1
+        assert info.status == 1, info.status
+        key = (int(scales[i]), which[i])
+        if want is not None:
+            assert info.count == want[key], (key, info.count, want[key])
+            checked += 1
         ms = (info.done_ns - info.submit_ns) / 1e6
         lat.append(ms)
         stages["queue"].append((info.load_ns - info.submit_ns) / 1e6)
@@ -424,39 +467,94 @@ def run_serve(args):
             lat18.append(ms)
         by_scale.setdefault(int(scales[i]), []).append(
             (ms, (info.ready_ns - info.load_ns) / 1e6, (info.done_ns - info.launch_ns) / 1e6))
-        trace.append((int(scales[i]), int(picks[i][0].m), info.submit_ns, info.load_ns, info.ready_ns, info.launch_ns,
-                      info.done_ns, info.batch))
-        edges += picks[i][0].m
+        if trace is not None:
+            trace.append((int(scales[i]), int(pool[key[0]][key[1]][0].m), info.submit_ns, info.load_ns,
+                          info.ready_ns, info.launch_ns, info.done_ns, info.batch))
+        edges += pool[key[0]][key[1]][0].m
         first_sub = info.submit_ns if first_sub is None else min(first_sub, info.submit_ns)
         last_done = max(last_done, info.done_ns)
         srv.release(ids[i])
     th.join()
-    stats = srv.stats()
-    srv.close()
+    span = (last_done - first_sub) / 1e9
+    return {"rate": rate, "duration_s": duration, "requests": n_req, "value": edges / span, "unit": UNIT,
+            "requests_per_s": n_req / span, "oracle_checked": checked,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "p50_scale_le_18": float(np.percentile(lat18, 50)) if lat18 else None,
+                           "p99_scale_le_18": float(np.percentile(lat18, 99)) if lat18 else None,
+                           "n_scale_le_18": len(lat18),
+                           "definition": "bbtc_submit -> count in host memory (server steady clock)"},
+            "stages_ms_p50_p99": {k: [float(np.percentile(v, 50)), float(np.percentile(v, 99))]
+                                  for k, v in stages.items()},
+            "by_scale_p50_ms": {s: {"n": len(v), "latency": float(np.percentile([x[0] for x in v], 50)),
+                                    "load": float(np.percentile([x[1] for x in v], 50)),
+                                    "count": float(np.percentile([x[2] for x in v], 50))}
+                                for s, v in sorted(by_scale.items())}}
+
+
+def measure_serve(max_scale: int, rates, duration: float, loaders: int, pin: bool, copy_engine_uploads: bool,
+                  check: bool = True, trace=None) -> dict:
+    """Pool generation, oracle counts of every pool graph, one warm-up
+    request per scale, then one Poisson stream per rate on the same server."""
+    from bbtc_b200 import Server
+    t0 = time.time()
+    pool, keep = serve_pool(max_scale, pin)
+    gen_s = time.time() - t0
+    t0 = time.time()
+    want = None
+    if check:
+        items = [(g, c) for s in sorted(pool) for g, c in pool[s]]
+        keys = [(s, j) for s in sorted(pool) for j in range(len(pool[s]))]
+        want = dict(zip(keys, oracle_counts(items)))
+    oracle_s = time.time() - t0
+    srv = Server(0, loaders=loaders, copy_engine_uploads=copy_engine_uploads)
+    try:
+        for s in sorted(pool):
+            g, c = pool[s][0]
+            info = srv.wait(srv.submit_csr(g, c))
+            assert want is None or info.count == want[(s, 0)]
+        runs = [serve_once(srv, pool, max_scale, r, duration, seed=7 + k, want=want, trace=trace)
+                for k, r in enumerate(rates)]
+        st = srv.stats()
+    finally:
+        srv.close()
+    del keep
+    return {"runs": runs, "pool_graphs": sum(len(v) for v in pool.values()), "generate_s": round(gen_s, 1),
+            "oracle_s": round(oracle_s, 1), "launches": st.launches, "max_batch": st.max_batch,
+            "loaders": loaders, "pinned_requests": pin,
+            "small_uploads": "copy engines" if copy_engine_uploads or not pin else "kernel reads",
+            "workload": f"serving: Poisson arrivals, R-MAT scale 12+Geom(0.3) <= {max_scale}, ef 16"}
+
+
+def run_serve(args):
+    rates = [float(x) for x in args.rates.split(",")] if args.rates else [args.rate]
+    trace = [] if args.trace else None
+    sv = measure_serve(args.serve_max_scale, rates, args.duration, args.loaders, bool(args.pin),
+                       args.copy_engine_uploads, check=not args.no_check, trace=trace)
     if args.trace:
         with open(args.trace, "w") as f:
             json.dump({"fields": ["scale", "m", "submit_ns", "load_ns", "ready_ns", "launch_ns", "done_ns", "batch"],
                        "requests": trace}, f)
-    span = (last_done - first_sub) / 1e9
-    res = {"metric": METRIC, "value": edges / span, "unit": UNIT, "n_gpus": 1, "steps": n_req, "warmup": len(pool),
-           "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "u32", "data": "synthetic",
-           "config": {"workload": f"serving: Poisson {args.rate:g} req/s for {args.duration:g} s, R-MAT scale "
-                                  f"12+Geom(0.3) <= {args.serve_max_scale}, ef 16", "requests": n_req,
-                      "generate_s": round(gen_s, 1), "launches": stats.launches, "max_batch": stats.max_batch,
-                      "loaders": args.loaders, "pinned_requests": bool(pinned),
-                      "small_uploads": "copy engines" if args.copy_engine_uploads or not pinned else "kernel reads"},
-           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                          "p50_scale_le_18": float(np.percentile(lat18, 50)) if lat18 else None,
-                          "p99_scale_le_18": float(np.percentile(lat18, 99)) if lat18 else None,
-                          "definition": "bbtc_submit -> count in host memory (server steady clock)"},
-           "stages_ms_p50_p99": {k: [float(np.percentile(v, 50)), float(np.percentile(v, 99))]
-                                 for k, v in stages.items()},
-           "by_scale_p50_ms": {s: {"n": len(v), "latency": float(np.percentile([x[0] for x in v], 50)),
-                                   "load": float(np.percentile([x[1] for x in v], 50)),
-                                   "count": float(np.percentile([x[2] for x in v], 50))}
-                               for s, v in sorted(by_scale.items())}}
-    print(json.dumps(res), flush=True)
+    peak = max(r["value"] for r in sv["runs"])
+    for r in sv["runs"]:
+        res = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": r["requests"],
+               "warmup": sv["pool_graphs"], "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+               "config": {"workload": f"{sv['workload']}, {r['rate']:g} req/s for {r['duration_s']:g} s",
+                          **{k: v for k, v in sv.items() if k not in ("runs", "workload")}},
+               **{k: v for k, v in r.items() if k not in ("value", "unit")},
+               "frac_of_sweep_peak": r["value"] / peak}
+        print(json.dumps(res), flush=True)
+
+
+def child_line(extra) -> dict | None:
+    """Run this script with `extra` arguments in a child process and return
+    its last JSON line (None, with the error, if it failed)."""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), *extra], capture_output=True, text=True,
+                       timeout=1200)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": f"exit {r.returncode}: {r.stderr.strip()[-400:]}"}
+    return json.loads(lines[-1])
 
 
 def main():
@@ -630,6 +728,40 @@ def main():
                              "the reference's sources)",
                    "seconds": secs[0], "count_matches_gpu": ref_match}
 
+    # --- the reference's own GPU executable (its one-launch-per-task form), same graph ---
+    ref_gpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        import oracle
+        if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "bbtc_gpu")):
+            try:
+                part = "pal" if args.partitioner.startswith("pal") else args.partitioner
+                r = oracle.ref_gpu_cli(g.n, g.indptr, g.indices, part, args.ncut, repeat=3, timeout=900)
+                tr = statistics.median(r["count_seconds"])
+                ref_gpu = {"value": g.m / tr, "unit": UNIT, "ms_per_step": tr * 1e3, "triangles": r["triangles"],
+                           "count_matches_gpu": r["triangles"] == count, "copy_s": r["copy_seconds"],
+                           "layout_s": r["layout_seconds"], "over_reference_gpu": tr / t_mean,
+                           "run": "oracle/_ref/bbtc_gpu (the reference's src/bbtc.cu built unmodified for "
+                                  "sm_100a) --ngpu 1 --border -1 --copy-first --repeat 3, its own SARMA cuts; "
+                                  "median 'Triangle Counting Execution Time'"}
+            except Exception as e:  # the baseline is reported, not required
+                ref_gpu = {"error": str(e)[-300:]}
+
+    # --- batched launch and serving sub-records (the BASELINE batching and serving configurations, short) ---
+    # each in a fresh child process, as a deployment runs them (host threads and
+    # device memory pools of this process do not carry over)
+    batch_rec = serve_rec = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batch_rec = child_line(["--config", "batch", "--batch-max-scale", str(args.sub_batch_max_scale),
+                                "--steps", "5", "--warmup", "2", "--batch-plain-steps", "0"])
+    if rank == 0 and world == 1 and not args.no_serve:
+        rate = args.sub_serve_rate or (0.8 * SERVE_PEAK_RPS)
+        serve_rec = child_line(["--config", "serve", "--rate", f"{rate:g}", "--duration",
+                                f"{args.sub_serve_duration:g}", "--serve-max-scale", "22"])
+        if serve_rec is not None:
+            serve_rec.update({"peak_rps": SERVE_PEAK_RPS, "rate_over_peak": rate / SERVE_PEAK_RPS,
+                              "peak_note": "SERVE_PEAK_RPS: the request rate where edges/s stopped growing in "
+                                           "`bench.py --config serve --rates ...` (profiles/serving_sweep.md)"})
+
     peak, peak_kind = peaks()
     fb = g.fused_bytes(cuts) if args.kernel in ("auto", "fused") else None
     model_bytes = fb["bytes"] if fb else balg
@@ -669,6 +801,9 @@ def main():
                               "which this kernel does not read. dram_gbs: ncu DRAM traffic of one launch over the "
                               "same time" + (f"; traffic: {traffic_note}" if traffic_note else ""))},
         "cpu_baseline": cpu,
+        "reference_gpu": ref_gpu,
+        "batch": batch_rec,
+        "serve": serve_rec,
         "gpu_launches": launches,
         "clocks": clk,
         "triangles_per_sec": (count / t_mean) if world == 1 else None,
