@@ -125,6 +125,7 @@ void graph_release_on(bbtc_graph* g, cudaStream_t s) {
   if (g->d_indices) cudaFreeAsync(g->d_indices, s);
   if (g->d_words) cudaFreeAsync(g->d_words, s);
   if (g->d_wptr) cudaFreeAsync(g->d_wptr, s);
+  if (g->d_desc) cudaFreeAsync(g->d_desc, s);
   if (g->d_count) cudaFreeAsync(g->d_count, s);
   delete g;
 }
@@ -270,6 +271,7 @@ int bbtc_graph_free(bbtc_graph* g) {
   if (g->d_indices) cudaFreeAsync(g->d_indices, s);
   if (g->d_words) cudaFreeAsync(g->d_words, s);
   if (g->d_wptr) cudaFreeAsync(g->d_wptr, s);
+  if (g->d_desc) cudaFreeAsync(g->d_desc, s);
   if (g->d_count) cudaFreeAsync(g->d_count, s);
   cudaStreamSynchronize(s);
   delete g;

@@ -743,10 +743,9 @@ __global__ void __launch_bounds__(256, 4) k_count_task(const DevTask* __restrict
 struct FusedFrame {
   const uint32_t* rp;    // reversed tile (j, i): row pointers
   const uint2* rec;      // its forward-edge records
-  const uint32_t* gp;    // oriented CSR
-  const uint32_t* gi;
+  const uint4* desc;     // per vertex: row start, pair start, first id, last id
+  const uint32_t* gi;    // oriented CSR ids
   const uint2* gw;       // word-compressed rows
-  const uint32_t* wp;    // their row pointers
   uint32_t H, e1, b, ee; // rows, unit end, current row, end of the current row's entries
   uint32_t pivot_base, ps, pd, base, words, rlen, kind, slot;
   uint32_t ws, wn;       // the pivot row's word pairs
@@ -757,12 +756,12 @@ static_assert(sizeof(FusedFrame) <= (kSegWords - kFrameOffset) * sizeof(uint32_t
 enum : uint32_t { kNoPivot = 0xffffffffu };
 
 // Choose the pivot structure of row v (ids prow[0..pd)) and record it in the frame.
+// first / last: the row's first and last id.
 __device__ __forceinline__ void fused_choose(volatile FusedFrame* fr, const uint32_t* __restrict__ prow, uint32_t pd,
-                                             uint32_t wn, uint32_t bm_words, uint32_t lane) {
+                                             uint32_t wn, uint32_t first, uint32_t last, uint32_t bm_words,
+                                             uint32_t lane) {
   uint32_t kind = kNoPivot, base = 0, words = 0, rlen = 0;
   if (pd > 0) {
-    const uint32_t first = prow[0];
-    const uint32_t last = prow[pd - 1];
     const uint32_t span_words = (last >> 5) - (first >> 5) + 1;
     if (span_words < bm_words) {
       kind = kPivotBitmap;
@@ -871,9 +870,10 @@ __device__ __forceinline__ void fused_clear_rank(const uint2* __restrict__ pw, u
 template <uint32_t KIND>
 __device__ __forceinline__ void fused_clear_words(const uint2* __restrict__ pw, uint32_t wn, uint32_t base_w,
                                                   uint32_t words, uint32_t* bm, uint32_t lane) {
-  // up to 512 words (bitmap kind), or as many as the row has pairs, are
-  // cleared as a range (stores only); otherwise the row's words, read again
-  if ((KIND == kPivotBitmap && words <= 512) || wn >= words) {
+  // a bitmap with at least a third of its words set (or a split window as
+  // many words as the row has pairs) is cleared as a range, stores only;
+  // otherwise the row's words are read again and cleared one by one
+  if ((KIND == kPivotBitmap && 3 * wn >= words) || wn >= words) {
     for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
   } else {
     for (uint32_t i = lane; i < wn; i += 32) {
@@ -971,16 +971,16 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
       const uint32_t mid = (lo + hi) >> 1;
       if (prefix[mid] <= g) lo = mid; else hi = mid;
     }
+    const uint32_t first_unit = prefix[lo];
     if (lane == 0) {
       const DevTask* tk = tasks + lo;
-      const uint32_t e0 = (g - prefix[lo]) * tk->unit_edges;  // < nnz < 2^32
+      const uint32_t e0 = (g - first_unit) * tk->unit_edges;  // < nnz < 2^32
       const uint32_t nnz = tk->rows.nnz;
       fr->rp = tk->rows.rp;
       fr->rec = tk->rows.rec;
-      fr->gp = tk->g_indptr;
+      fr->desc = tk->g_desc;
       fr->gi = tk->g_indices;
       fr->gw = tk->g_words;
-      fr->wp = tk->g_wptr;
       fr->H = tk->rows.H;
       fr->e1 = nnz - e0 > tk->unit_edges ? e0 + tk->unit_edges : nnz;
       fr->b = tk->rows.erow[e0 >> 5];  // units start at multiples of 32 entries
@@ -1000,15 +1000,18 @@ __global__ void __launch_bounds__(256, MINB) k_fused_queue(const DevTask* __rest
         const uint32_t lo = fr->pivot_base;
         const uint32_t v = lo + b;
         const uint32_t* gi = fr->gi;
-        uint32_t ps = fr->gp[v];
-        uint32_t pd = fr->gp[v + 1] - ps;
-        uint32_t ws = fr->wp[v];
-        uint32_t wn = fr->wp[v + 1] - ws;
+        // the pivot row's extent in one pair of 16-byte loads
+        const uint4 d0 = fr->desc[v], d1 = fr->desc[v + 1];
+        uint32_t ps = d0.x, pd = d1.x - d0.x, ws = d0.y, wn = d1.y - d0.y;
+        uint32_t first = d0.z;
         uint32_t mask0 = FULL;
         // ids of N+(v) below the task columns (never, for a CSR oriented from
         // lower to higher ids) are left out of the pivot
-        if (pd > 0 && gi[ps] < lo) pivot_suffix(gi, (const uint2*)fr->gw, lo, ps, pd, ws, wn, mask0);
-        fused_choose(fr, gi + ps, pd, wn, bm_words, lane);
+        if (pd > 0 && first < lo) {
+          pivot_suffix(gi, (const uint2*)fr->gw, lo, ps, pd, ws, wn, mask0);
+          if (pd > 0) first = gi[ps];
+        }
+        fused_choose(fr, gi + ps, pd, wn, first, d0.w, bm_words, lane);
         if (lane == 0) {
           fr->ee = ee;
           fr->ps = ps;
@@ -1152,6 +1155,7 @@ static int make_plan(const std::vector<bbtc_graph*>& graphs, const std::vector<s
           d.g_indices = g->d_indices;
           d.g_words = reinterpret_cast<const uint2*>(g->d_words);
           d.g_wptr = g->d_wptr;
+          d.g_desc = static_cast<const uint4*>(g->d_desc);
           d.pivot_base = g->cuts[j];
           add(d, 0.5 * part_row_len(g, i));
           if (!o.unit_work) list.back().unit_edges = 0;  // set below from the request's size
@@ -1293,20 +1297,17 @@ int staging_status(bbtc_ctx* ctx) {
 }
 
 // Options left at 0 ("auto") resolved for the request's graphs.  The
-// bitmap: 1024 words per warp, 2048 once a graph has 2^24 vertices or more
-// (R-MAT s22: 8.8 ms with 1024 against 10.7 with 2048; s24: 71 ms with 2048
-// against 114 with 1024 -- the wider id space puts more of each pivot row
-// outside a 1024-word window).  Occupancy: fused task rows 6 blocks per SM
-// (40 registers) while the bitmap leaves shared memory for them, else 4 (64
-// registers); per-task kernels 4 (R-MAT s20: bitmap 10.4 ms at 4 against
+// bitmap: 1024 words per warp.  Rows wider than that run as rank bitmaps,
+// so a larger buffer only costs occupancy (one B200, ms per count, 512 / 768
+// / 1024 / 1536 / 2048 words: R-MAT s22 7.92 / 7.63 / 7.49 / 8.16 / 9.56;
+// s24 - / - / 41.8 / 46.5 / 56.5).  Occupancy: fused task rows 6 blocks per
+// SM (40 registers) while the bitmap leaves shared memory for them, else 4
+// (64 registers); per-task kernels 4 (R-MAT s20: bitmap 10.4 ms at 4 against
 // 12.4 at 6, search 14.4 / 15.7, merge 27.5 / 31.5).
 static bbtc_opts resolve_opts(const std::vector<bbtc_graph*>& graphs, const bbtc_opts& in, bool fused) {
   bbtc_opts o = in;
-  if (!o.bitmap_words) {
-    uint32_t n = 0;
-    for (const bbtc_graph* g : graphs) n = std::max(n, g->n);
-    o.bitmap_words = n >= (1u << 24) ? 2048 : 1024;
-  }
+  (void)graphs;
+  if (!o.bitmap_words) o.bitmap_words = 1024;
   if (!o.occupancy) o.occupancy = fused && norm_bm_words(o.bitmap_words) <= 1024 ? 6 : 4;
   return o;
 }

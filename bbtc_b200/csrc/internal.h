@@ -107,6 +107,7 @@ struct DevTask {
   const uint32_t* g_indices;
   const uint2* g_words;       // fused: word-compressed rows
   const uint32_t* g_wptr;     // fused: their row pointers (n + 1)
+  const uint4* g_desc;        // fused: per vertex (row start, pair start, first id, last id), n + 1
   uint32_t pivot_base;        // fused: first vertex id of part j
   uint32_t kind;
   uint32_t unit_edges;  // entries of `rows` per work unit
@@ -217,6 +218,7 @@ struct bbtc_graph {
   uint32_t* d_indices = nullptr;
   void* d_words = nullptr;        // word-compressed rows: (word, mask) uint2 pairs
   uint32_t* d_wptr = nullptr;     // n + 1 pair offsets
+  void* d_desc = nullptr;         // n + 1 pivot descriptors (uint4): row start, pair start, first id, last id
   bbtc::BlockTiles fwd, rev;
   uint64_t* d_count = nullptr;  // result slot
   uint64_t device_bytes = 0;

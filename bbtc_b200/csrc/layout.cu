@@ -92,9 +92,12 @@ __global__ void k_validate_rows(const uint32_t* __restrict__ indptr, uint32_t n,
 }
 
 // Expands the row id of every edge and checks ids; rows whose pointers are
-// out of order or past m are skipped (k_validate_rows flags them).
+// out of order or past m are skipped (k_validate_rows flags them).  With
+// `flags`, also marks the edges that open a new 32-id word of their row
+// (flags[e] = 1), the input of the word-compressed rows.
 __global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
-                               uint32_t n, uint64_t m, uint32_t* __restrict__ rows, uint32_t* __restrict__ bad) {
+                               uint32_t n, uint64_t m, uint32_t* __restrict__ rows, uint32_t* __restrict__ bad,
+                               uint32_t* __restrict__ flags) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -104,8 +107,10 @@ __global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32
     for (uint32_t e = a + lane; e < b; e += 32) {
       rows[e] = u;
       const uint32_t c = indices[e];
+      const uint32_t prev = e > a ? indices[e - 1] : 0u;
       if (c >= n) atomicOr(bad, 8u);
-      if (e > a && indices[e - 1] >= c) atomicOr(bad, 16u);
+      if (e > a && prev >= c) atomicOr(bad, 16u);
+      if (flags) flags[e] = (e == a || (c >> 5) != (prev >> 5)) ? 1u : 0u;
     }
   }
 }
@@ -299,45 +304,38 @@ __global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint3
       // forward edge fe = (c -> u) of this reversed entry: the pairs of row c
       // from the record's first pair to the row's end
       const uint32_t fe = eids[e];
-      rec[pos] = make_uint2(record_start(fptr, fidx, words, wptr, u, c, cuts[x], wpos[fe]), wptr[c + 1]);
+      rec[pos] = make_uint2(record_start(fptr, fidx, words, wptr, u, c, cuts[x], wpos[fe] - 1u), wptr[c + 1]);
     }
   }
 }
 
 // Word-compressed rows: each row's ids grouped by 32-id word into (word, bit
-// mask) pairs.  flags[e] = 1 when edge e opens a new word of its row.
-__global__ void k_word_flags(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
-                             const uint32_t* __restrict__ rows, uint64_t m, uint32_t* __restrict__ flags) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride)
-    flags[e] = (e == indptr[rows[e]] || (indices[e] >> 5) != (indices[e - 1] >> 5)) ? 1u : 0u;
-}
-
-// After an inclusive scan of the flags, wpos[e] - 1 is the pair edge e lands in
-// (k_word_index turns the scan into that index).
-__global__ void k_word_index(uint32_t* __restrict__ wpos, uint64_t m) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) wpos[e] -= 1;
-}
-
-// wpos[e]: the pair edge e lands in.
+// mask) pairs.  flags[e] = 1 when edge e opens a new word of its row
+// (k_expand_check); wpos = their inclusive scan, so edge e lands in pair
+// wpos[e] - 1.
 __global__ void k_word_fill(const uint32_t* __restrict__ indices, const uint32_t* __restrict__ flags,
                             const uint32_t* __restrict__ wpos, uint64_t m, uint2* __restrict__ words) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
     const uint32_t x = indices[e];
-    const uint32_t p = wpos[e];
+    const uint32_t p = wpos[e] - 1u;
     if (flags[e]) words[p].x = x >> 5;
     atomicOr(&words[p].y, 1u << (x & 31));
   }
 }
 
 // wptr[u] = first pair of row u (u in [0, n]); a row's first edge opens a pair.
-__global__ void k_word_rowptr(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ wpos, uint32_t n,
-                              uint64_t m, uint32_t* __restrict__ wptr) {
+// desc[u]: the fused kernel's view of row u as a pivot, in one 16-byte load.
+__global__ void k_word_rowptr(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+                              const uint32_t* __restrict__ wpos, uint32_t n, uint64_t m, uint32_t* __restrict__ wptr,
+                              uint4* __restrict__ desc) {
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= n; u += gridDim.x * blockDim.x) {
     const uint32_t e = indptr[u];
-    wptr[u] = (uint64_t)e < m ? wpos[e] : (m ? wpos[m - 1] + 1 : 0u);
+    const uint32_t w = (uint64_t)e < m ? wpos[e] - 1u : (m ? wpos[m - 1] : 0u);
+    wptr[u] = w;
+    // pivot descriptor: row start, pair start, first and last id (0, 0 for an empty row)
+    const bool has = u < n && indptr[u + 1] > e;
+    desc[u] = make_uint4(e, w, has ? indices[e] : 0u, has ? indices[indptr[u + 1] - 1] : 0u);
   }
 }
 
@@ -641,7 +639,9 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   const uint32_t* d_indptr = g->d_indptr;
   const uint32_t* d_indices = g->d_indices;
 
-  DevBuf d_cuts, bad, rows, stats_r, coloff_r;
+  DevBuf d_cuts, bad, rows, stats_r, coloff_r, wflags, wpos;
+  BBTC_TRY(dalloc(wflags, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(wpos, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(d_cuts, g->cuts.size() * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(bad, sizeof(uint32_t), s));
   BBTC_TRY(dalloc(rows, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
@@ -658,7 +658,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     // both checks, one read-back: nothing indexes by the input before it passes
     k_validate_rows<<<grid, 256, 0, s>>>(d_indptr, n, m, bad.as<uint32_t>());
     BBTC_CUDA(cudaGetLastError());
-    k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>());
+    k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>(),
+                                        wflags.as<uint32_t>());
     BBTC_CUDA(cudaGetLastError());
     uint32_t* hb = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageBad);
     BBTC_CUDA(cudaMemcpyAsync(hb, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -678,33 +679,28 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   // the forward block CSR waits until something needs it (ensure_fwd): the
   // fused task rows read only the reversed one
 
-  // word-compressed rows (the fused task rows stream these)
-  DevBuf wflags, wpos;
-  BBTC_TRY(dalloc(wflags, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
-  BBTC_TRY(dalloc(wpos, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+  // word-compressed rows (the fused task rows stream these); k_expand_check wrote the flags
   {
     cudaError_t e1 = dev_malloc(&g->d_words, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s);
     cudaError_t e2 = dev_malloc(&g->d_wptr, ((size_t)n + 1) * sizeof(uint32_t), s);
-    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+    cudaError_t e3 = dev_malloc(&g->d_desc, ((size_t)n + 1) * sizeof(uint4), s);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
       cudaGetLastError();
       return fail(BBTC_ERR_NOMEM, "device allocation of the word-compressed rows failed");
     }
     BBTC_TRY(zero_fill(g->d_words, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s, grid));
     if (m > 0) {
-      k_word_flags<<<grid, 256, 0, s>>>(d_indptr, d_indices, rows.as<uint32_t>(), m, wflags.as<uint32_t>());
-      BBTC_CUDA(cudaGetLastError());
       size_t tb = 0;
       BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, wflags.as<uint32_t>(), wpos.as<uint32_t>(), (int64_t)m, s));
       DevBuf tmp;
       BBTC_TRY(dalloc(tmp, tb, s));
       BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, wflags.as<uint32_t>(), wpos.as<uint32_t>(), (int64_t)m, s));
-      k_word_index<<<grid, 256, 0, s>>>(wpos.as<uint32_t>(), m);
-      BBTC_CUDA(cudaGetLastError());
       k_word_fill<<<grid, 256, 0, s>>>(d_indices, wflags.as<uint32_t>(), wpos.as<uint32_t>(), m,
                                        reinterpret_cast<uint2*>(g->d_words));
       BBTC_CUDA(cudaGetLastError());
     }
-    k_word_rowptr<<<grid, 256, 0, s>>>(d_indptr, wpos.as<uint32_t>(), n, m, g->d_wptr);
+    k_word_rowptr<<<grid, 256, 0, s>>>(d_indptr, d_indices, wpos.as<uint32_t>(), n, m, g->d_wptr,
+                                       static_cast<uint4*>(g->d_desc));
     BBTC_CUDA(cudaGetLastError());
   }
 
@@ -750,7 +746,7 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   BBTC_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   g->layout_ms = ms;
   g->device_bytes = block_bytes(g->rev, true) + ((uint64_t)n + 1 + m) * sizeof(uint32_t) + 64 * sizeof(uint64_t) +
-                    m * sizeof(uint2) + ((uint64_t)n + 1) * sizeof(uint32_t);
+                    m * sizeof(uint2) + ((uint64_t)n + 1) * (sizeof(uint32_t) + sizeof(uint4));
   return BBTC_OK;
 }
 
@@ -778,7 +774,8 @@ int build_fwd(bbtc_graph* g) {
   if (n > 0) {
     // row id of every edge (the CSR passed validation when it was uploaded)
     BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
-    k_expand_check<<<grid, 256, 0, s>>>(g->d_indptr, g->d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>());
+    k_expand_check<<<grid, 256, 0, s>>>(g->d_indptr, g->d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>(),
+                                        nullptr);
     BBTC_CUDA(cudaGetLastError());
   }
   BBTC_TRY(build_block(ctx, g->fwd, g->d_indptr, g->d_indices, rows.as<uint32_t>(), n, m, g->cuts,
@@ -825,7 +822,8 @@ int bbtc_graph_validate(const bbtc_graph* g) {
     if (words) BBTC_CUDA(cudaMemcpyAsync(h.data(), d, words * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     return BBTC_OK;
   };
-  std::vector<uint32_t> indptr, indices, wptr, pairs;
+  std::vector<uint32_t> indptr, indices, wptr, pairs, desc;
+  BBTC_TRY(get(desc, g->d_desc, 4 * ((uint64_t)n + 1)));
   BBTC_TRY(get(indptr, g->d_indptr, (uint64_t)n + 1));
   BBTC_TRY(get(indices, g->d_indices, mm));
   BBTC_TRY(get(wptr, g->d_wptr, (uint64_t)n + 1));
@@ -835,6 +833,7 @@ int bbtc_graph_validate(const bbtc_graph* g) {
   check::Words w{wptr.data(), pairs.data(), mm};
   std::string why = check::csr(c);
   if (why.empty()) why = check::words(c, w);
+  if (why.empty()) why = check::descs(c, w, desc.data());
   std::vector<uint32_t> tp, tc;
   if (why.empty()) check::transpose(c, tp, tc);
   const check::Csr tr{n, m, tp.data(), tc.data()};

@@ -11,6 +11,8 @@
 //   * the word-compressed rows: wptr[0] = 0, non-decreasing; within a row the
 //     32-id words strictly increase, masks are non-zero, and the pairs expand
 //     to exactly the row's ids;
+//   * the pivot descriptors: per vertex its row start, pair start, first and
+//     last id;
 //   * each block CSR (forward: rows of part x, columns of part y; reversed:
 //     the same with the transposed graph): row-pointer segments start on
 //     16-byte boundaries, stay inside the pool and do not overlap; a tile's
@@ -111,6 +113,19 @@ inline std::string words(const Csr& g, const Words& w) {
       }
     }
     if (e != end) return at("pairs miss ids of row", u);
+  }
+  return "";
+}
+
+// Pivot descriptors (4 words per vertex u <= n): row start, pair start,
+// first id and last id of row u (0, 0 for an empty row and for u = n).
+inline std::string descs(const Csr& g, const Words& w, const uint32_t* desc) {
+  for (uint32_t u = 0; u <= g.n; u++) {
+    const uint32_t* d = desc + 4 * (uint64_t)u;
+    const bool has = u < g.n && g.indptr[u + 1] > g.indptr[u];
+    const uint32_t first = has ? g.indices[g.indptr[u]] : 0, last = has ? g.indices[g.indptr[u + 1] - 1] : 0;
+    if (d[0] != g.indptr[u] || d[1] != w.wptr[u] || d[2] != first || d[3] != last)
+      return at("pivot descriptor differs from the row, vertex", u);
   }
   return "";
 }

@@ -174,7 +174,7 @@ typedef enum bbtc_kernel {
 typedef struct bbtc_opts {
   int mode;                  /* bbtc_mode */
   int kernel;                /* bbtc_kernel */
-  uint32_t bitmap_words;     /* shared bitmap / list words per warp: 0 = by graph size (1024; 2048 from 2^24 vertices) */
+  uint32_t bitmap_words;     /* shared bitmap / list words per warp: 0 = default (1024) */
   uint32_t warps_per_block;  /* 0 = default (8) */
   uint32_t unit_work;        /* target probes per work unit, 0 = default (256 task rows, 8192 tasks) */
   uint32_t blocks_per_sm;    /* persistent grid = SMs x this, 0 = occupancy limit */

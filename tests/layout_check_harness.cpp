@@ -174,6 +174,16 @@ int main(int argc, char** argv) {
   Csr tr{n, m, tp.data(), tc.data()};
   Built fwd = build(g, P, cuts, nullptr);
   Built rev = build(tr, P, cuts, &w, &g);
+  // pivot descriptors: row start, pair start, first id, last id
+  std::vector<uint32_t> desc(4 * ((size_t)n + 1), 0);
+  for (uint32_t u = 0; u <= n; u++) {
+    desc[4 * u] = indptr[u];
+    desc[4 * u + 1] = wptr[u];
+    if (u < n && indptr[u + 1] > indptr[u]) {
+      desc[4 * u + 2] = indices[indptr[u]];
+      desc[4 * u + 3] = indices[indptr[u + 1] - 1];
+    }
+  }
 
   uint32_t t = 0, row = 0;
   auto entry = [&](Built& b, uint32_t len) -> uint64_t {
@@ -248,12 +258,19 @@ int main(int argc, char** argv) {
   } else if (fault == "rec_end") {
     const uint64_t p = entry(rev, 1);
     rev.rec[2 * p + 1] += 1;
+  } else if (fault == "desc_last") {
+    for (uint32_t u = 0; u < n; u++)
+      if (indptr[u + 1] > indptr[u]) {
+        desc[4 * u + 3] += 1;
+        break;
+      }
   } else {
     return 2;
   }
 
   std::string why = csr(g);
   if (why.empty()) why = words(g, w);
+  if (why.empty()) why = descs(g, w, desc.data());
   if (why.empty()) why = tiles("reversed tiles", tr, view(rev, P, cuts), w);
   if (why.empty()) why = tiles("forward tiles", g, view(fwd, P, cuts), w);
   std::printf("%s\n", why.empty() ? "OK" : why.c_str());

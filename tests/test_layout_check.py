@@ -29,6 +29,7 @@ FAULTS = {
     "erow": "row index names the wrong row",
     "rec_pair": "record",
     "rec_end": "record outside the row's pairs",
+    "desc_last": "pivot descriptor differs",
 }
 
 
