@@ -21,6 +21,7 @@ struct AdmitLimits {
   uint64_t now_ns;
   bool small_only;       // the loader takes small requests only
   size_t scan_limit;     // pending requests looked at
+  bool large_ok = true;  // false: as many large requests are loading as the server allows at once
 };
 
 // Index in `pending` (a random-access sequence of pointers to objects with
@@ -32,7 +33,7 @@ size_t admit_pick(const Seq& pending, const AdmitLimits& lim) {
   const size_t n = pending.size() < lim.scan_limit ? pending.size() : lim.scan_limit;
   for (size_t i = 0; i < n; i++) {
     const auto* r = pending[i];
-    if (lim.small_only && r->m > lim.small_edges) continue;
+    if ((lim.small_only || !lim.large_ok) && r->m > lim.small_edges) continue;
     const bool never = r->reserved > lim.budget;
     if (!never && lim.in_use + r->reserved > lim.budget && lim.in_use != 0) continue;
     if (lim.now_ns - r->t_submit >= lim.aging_ns) return i;

@@ -1103,6 +1103,7 @@ int kernel_smem_optin(bbtc_ctx* ctx, const bbtc_opts& o) {
   BBTC_CUDA(cudaFuncSetAttribute(k_count_queue<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_fused_queue<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   BBTC_CUDA(cudaFuncSetAttribute(k_count_task, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   ctx->smem_set = sm;
@@ -1261,9 +1262,11 @@ static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint6
       plan->launches++;
     }
   } else {
-    // the register budget: 4, 6 (default) or 8 resident blocks per SM
-    const uint32_t occ = o.occupancy >= 8 ? 8 : (o.occupancy >= 6 ? 6 : 4);
-    auto* fkern = occ == 8 ? k_fused_queue<8> : (occ == 6 ? k_fused_queue<6> : k_fused_queue<4>);
+    // the register budget: 4, 5, 6 or 8 resident blocks per SM (the per-task
+    // queue kernel has no 5-block variant and runs 4 there)
+    const uint32_t occ = o.occupancy >= 8 ? 8 : (o.occupancy >= 6 ? 6 : (o.occupancy == 5 ? 5 : 4));
+    auto* fkern = occ == 8 ? k_fused_queue<8>
+                           : (occ == 6 ? k_fused_queue<6> : (occ == 5 ? k_fused_queue<5> : k_fused_queue<4>));
     auto* qkern = occ == 8 ? k_count_queue<8> : (occ == 6 ? k_count_queue<6> : k_count_queue<4>);
     int per_sm = 0;
     if (plan->fused)

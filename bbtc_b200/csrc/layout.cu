@@ -116,10 +116,13 @@ __global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32
 }
 
 // Run lengths: the first edge of each (row, tile) run writes the length into
-// slot (rp_off[tile] + local row + 1) of the counts buffer.
+// slot (rp_off[tile] + local row + 1) of the counts buffer.  runs[e] = e for
+// the first edge of a run, else 0: its inclusive max-scan gives every edge
+// the start of its run.
 __global__ void k_entry_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
                               const uint32_t* __restrict__ rows, uint64_t m, const uint32_t* __restrict__ cuts_g,
-                              uint32_t P, const uint64_t* __restrict__ rp_off, uint32_t* __restrict__ counts) {
+                              uint32_t P, const uint64_t* __restrict__ rp_off, uint32_t* __restrict__ counts,
+                              uint32_t* __restrict__ runs) {
   __shared__ uint32_t cuts[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
   __syncthreads();
@@ -129,7 +132,9 @@ __global__ void k_entry_count(const uint32_t* __restrict__ indptr, const uint32_
     const uint32_t c = indices[e];
     const uint32_t y = part_of(cuts, P, c);
     const uint32_t a = indptr[u];
-    if (e > a && indices[e - 1] >= cuts[y]) continue;  // not the first edge of its run
+    const bool first = e == a || indices[e - 1] < cuts[y];
+    runs[e] = first ? (uint32_t)e : 0u;
+    if (!first) continue;
     const uint32_t end = lower_bound_range(indices, (uint32_t)e, indptr[u + 1], cuts[y + 1]);
     const uint32_t x = part_of(cuts, P, u);
     counts[rp_off[x * P + y] + (u - cuts[x]) + 1] = end - (uint32_t)e;
@@ -278,7 +283,7 @@ __device__ __forceinline__ uint32_t record_start(const uint32_t* __restrict__ fp
 // Scatter tile-local column ids (and, for the reversed graph, the records of
 // the forward edges) into the column pool.  For the reversed graph
 // `fptr` / `fidx` / `words` are the oriented CSR and its word-compressed rows.
-__global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+__global__ void k_entry_scatter(const uint32_t* __restrict__ runs, const uint32_t* __restrict__ indices,
                                 const uint32_t* __restrict__ rows, uint64_t m, const uint32_t* __restrict__ cuts_g,
                                 uint32_t P, const uint64_t* __restrict__ rp_off, const uint64_t* __restrict__ col_off,
                                 const uint32_t* __restrict__ rp, uint32_t* __restrict__ col,
@@ -296,8 +301,7 @@ __global__ void k_entry_scatter(const uint32_t* __restrict__ indptr, const uint3
     const uint32_t y = part_of(cuts, P, c);
     const uint32_t x = part_of(cuts, P, u);
     const uint32_t t = x * P + y;
-    const uint32_t a = indptr[u];
-    const uint32_t run = lower_bound_range(indices, a, (uint32_t)e, cuts[y]);
+    const uint32_t run = runs[e];  // first edge of this (row, tile) run
     const uint64_t pos = col_off[t] + rp[rp_off[t] + (u - cuts[x])] + ((uint32_t)e - run);
     col[pos] = c - cuts[y];
     if (rec) {
@@ -441,7 +445,8 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
     }
   }
   bt.stream = s;
-  DevBuf offs, counts, base;
+  DevBuf offs, counts, base, runs;
+  BBTC_TRY(dalloc(runs, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(offs, (T + P + 1) * sizeof(uint64_t), s));
   BBTC_TRY(dalloc(counts, bt.rp_len * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(base, T * sizeof(uint32_t), s));
@@ -458,8 +463,16 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   BBTC_TRY(zero_fill(bt.d_col, bt.col_len * sizeof(uint32_t), s, grid));
   BBTC_CUDA(cudaMemsetAsync(d_stats, 0, 4 * T * sizeof(uint32_t), s));
   if (m > 0) {
-    k_entry_count<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, counts.as<uint32_t>());
+    k_entry_count<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, counts.as<uint32_t>(),
+                                       runs.as<uint32_t>());
     BBTC_CUDA(cudaGetLastError());
+    size_t rb = 0;
+    BBTC_CUDA(cub::DeviceScan::InclusiveScan(nullptr, rb, runs.as<uint32_t>(), runs.as<uint32_t>(), cub::Max(),
+                                             (int64_t)m, s));
+    DevBuf rtmp;
+    BBTC_TRY(dalloc(rtmp, rb, s));
+    BBTC_CUDA(cub::DeviceScan::InclusiveScan(rtmp.p, rb, runs.as<uint32_t>(), runs.as<uint32_t>(), cub::Max(),
+                                             (int64_t)m, s));
   }
   size_t tmp_bytes = 0;
   BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, counts.as<uint32_t>(), bt.d_rp, (int64_t)bt.rp_len, s));
@@ -484,7 +497,7 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
     BBTC_CUDA(cudaGetLastError());
   }
   if (m > 0) {
-    k_entry_scatter<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
+    k_entry_scatter<<<grid, 256, 0, s>>>(runs.as<uint32_t>(), d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
                                          bt.d_col, eids, wpos, wptr, reinterpret_cast<uint2*>(bt.d_rec), fptr, fidx,
                                          words);
     BBTC_CUDA(cudaGetLastError());

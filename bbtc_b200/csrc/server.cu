@@ -40,6 +40,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <cuda.h>
+
 #include "admission.hpp"
 #include "internal.h"
 
@@ -121,8 +123,11 @@ struct bbtc_server {
   uint64_t next_id = 1;
   uint64_t in_use = 0;
   uint32_t loading = 0;
+  uint32_t loading_large = 0;  // large requests being uploaded / laid out
   bool stop = false;
   std::vector<std::thread> loaders;
+  CUgreenCtx green[2] = {nullptr, nullptr};  // SM partitions (small_sms > 0): small requests, large requests
+  uint32_t green_sms[2] = {0, 0};
   // statistics
   uint64_t counted = 0, max_batch_seen = 0;
 };
@@ -136,8 +141,9 @@ uint32_t lane_of(const bbtc_server* s, const Request* r) { return r->m <= s->opt
 
 // The next request a loader takes (admission.hpp), removed from `pending`, or nullptr.
 Request* pick(bbtc_server* s, bool small_only) {
-  const AdmitLimits lim{s->opts.hbm_budget, s->in_use, s->opts.small_edges,
-                        (uint64_t)s->opts.aging_ms * 1000000ull, now_ns(), small_only, kPickScan};
+  AdmitLimits lim{s->opts.hbm_budget, s->in_use, s->opts.small_edges,
+                  (uint64_t)s->opts.aging_ms * 1000000ull, now_ns(), small_only, kPickScan};
+  lim.large_ok = !s->opts.max_large_loads || s->loading_large < s->opts.max_large_loads;
   const size_t best = admit_pick(s->pending, lim);
   if (best == SIZE_MAX) return nullptr;
   Request* r = s->pending[best];
@@ -165,6 +171,8 @@ void loader_main(bbtc_server* s, bbtc_ctx* ctx_small, bbtc_ctx* ctx_large, bool 
     r->status = 1;
     r->t_load = now_ns();
     s->loading++;
+    const bool large = lane_of(s, r) == 1;
+    if (large) s->loading_large++;
     lk.unlock();
     bbtc_graph* g = nullptr;
     // a large layout runs on a low-priority stream with its grids capped, so
@@ -174,6 +182,7 @@ void loader_main(bbtc_server* s, bbtc_ctx* ctx_small, bbtc_ctx* ctx_large, bool 
                                      (uint32_t)r->cuts.size() - 1, &g);
     lk.lock();
     s->loading--;
+    if (large) s->loading_large--;
     if (rc != BBTC_OK) {
       s->in_use -= r->reserved;
       r->reserved = 0;
@@ -270,6 +279,78 @@ void launcher_main(bbtc_server* s, uint32_t lane) {
   plan.release();
 }
 
+// The driver's green-context calls (SM partitions), looked up once at the
+// version this library was built with; `ok` is false when the driver lacks
+// any of them.
+struct GreenApi {
+  CUresult (*get_device)(CUdevice*, int) = nullptr;
+  CUresult (*get_resource)(CUdevice, CUdevResource*, CUdevResourceType) = nullptr;
+  CUresult (*split)(CUdevResource*, unsigned*, const CUdevResource*, CUdevResource*, unsigned, unsigned) = nullptr;
+  CUresult (*gen_desc)(CUdevResourceDesc*, CUdevResource*, unsigned) = nullptr;
+  CUresult (*create)(CUgreenCtx*, CUdevResourceDesc, CUdevice, unsigned) = nullptr;
+  CUresult (*stream)(CUstream*, CUgreenCtx, unsigned, int) = nullptr;
+  CUresult (*destroy)(CUgreenCtx) = nullptr;
+  bool ok = false;
+};
+
+const GreenApi& green_api() {
+  static const GreenApi api = [] {
+    GreenApi a;
+    auto get = [](const char* name, void* fn) {
+      cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+      const bool found = cudaGetDriverEntryPointByVersion(name, static_cast<void**>(fn), CUDA_VERSION,
+                                                          cudaEnableDefault, &q) == cudaSuccess &&
+                         q == cudaDriverEntryPointSuccess;
+      cudaGetLastError();
+      return found;
+    };
+    a.ok = get("cuDeviceGet", &a.get_device) && get("cuDeviceGetDevResource", &a.get_resource) &&
+           get("cuDevSmResourceSplitByCount", &a.split) && get("cuDevResourceGenerateDesc", &a.gen_desc) &&
+           get("cuGreenCtxCreate", &a.create) && get("cuGreenCtxStreamCreate", &a.stream) &&
+           get("cuGreenCtxDestroy", &a.destroy);
+    return a;
+  }();
+  return api;
+}
+
+// Split the device's SMs into two green contexts: `small_sms` (rounded up by
+// the driver to its granularity, 8 on this architecture) for the small
+// requests, the rest for the large ones.  Kernels launched into a stream of
+// either run only on its SMs.
+int make_partitions(bbtc_server* s, uint32_t small_sms) {
+  const GreenApi& g = green_api();
+  if (!g.ok) return fail(BBTC_ERR_UNSUPPORTED, "the driver offers no green contexts (SM partitions)");
+  CUdevice dev = 0;
+  CUdevResource all{}, part{}, rest{};
+  unsigned groups = 1;
+  if (g.get_device(&dev, s->device) != CUDA_SUCCESS ||
+      g.get_resource(dev, &all, CU_DEV_RESOURCE_TYPE_SM) != CUDA_SUCCESS)
+    return fail(BBTC_ERR_CUDA, "reading the device's SM resource failed");
+  if (small_sms >= all.sm.smCount)
+    return fail(BBTC_ERR_ARG, "small_sms must leave SMs for the large requests");
+  if (g.split(&part, &groups, &all, &rest, 0, small_sms) != CUDA_SUCCESS || groups != 1 || rest.sm.smCount == 0)
+    return fail(BBTC_ERR_ARG, "the SMs could not be split into the requested partition");
+  CUdevResourceDesc d0 = nullptr, d1 = nullptr;
+  if (g.gen_desc(&d0, &part, 1) != CUDA_SUCCESS || g.gen_desc(&d1, &rest, 1) != CUDA_SUCCESS ||
+      g.create(&s->green[0], d0, dev, CU_GREEN_CTX_DEFAULT_STREAM) != CUDA_SUCCESS ||
+      g.create(&s->green[1], d1, dev, CU_GREEN_CTX_DEFAULT_STREAM) != CUDA_SUCCESS)
+    return fail(BBTC_ERR_CUDA, "creating the green contexts failed");
+  s->green_sms[0] = part.sm.smCount;
+  s->green_sms[1] = rest.sm.smCount;
+  return BBTC_OK;
+}
+
+// Move a context onto a stream of SM partition `p` (its grids are then sized to the partition's SMs).
+int set_partition_stream(bbtc_server* s, bbtc_ctx* c, int p, int priority) {
+  CUstream st = nullptr;
+  if (green_api().stream(&st, s->green[p], CU_STREAM_NON_BLOCKING, priority) != CUDA_SUCCESS)
+    return fail(BBTC_ERR_CUDA, "creating a stream in an SM partition failed");
+  cudaStreamDestroy(c->stream);
+  c->stream = reinterpret_cast<cudaStream_t>(st);
+  c->sms = (int)s->green_sms[p];
+  return BBTC_OK;
+}
+
 // Give a context's stream the requested priority (lower numbers run first).
 int set_stream_priority(bbtc_ctx* c, int priority) {
   cudaStream_t st = nullptr;
@@ -347,7 +428,7 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
     if (rc == BBTC_OK) s->load_ctx.push_back(c);
     if (rc == BBTC_OK) rc = set_stream_priority(c, i % 2 == 0 ? mid : lo);
     if (rc == BBTC_OK && i % 2 == 1) {
-      c->layout_blocks_per_sm = 2;
+      c->layout_blocks_per_sm = s->opts.large_layout_blocks_per_sm ? s->opts.large_layout_blocks_per_sm : 2;
       c->upload_window = 2;
     }
     // small requests from page-locked buffers are read by a kernel: their
@@ -355,6 +436,14 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
     // (p99 4.1 ms for a copy whose median is 0.03 ms)
     if (rc == BBTC_OK && i % 2 == 0 && !s->opts.copy_engine_uploads)
       c->zero_copy_bytes = 4 * std::max<uint64_t>(s->opts.small_edges, 1ull << 22) + 64;
+  }
+  if (rc == BBTC_OK && s->opts.small_sms) {
+    // lane 0 and every loader's small-request context on the small
+    // partition, lane 1 and the large-request contexts on the other
+    rc = make_partitions(s, s->opts.small_sms);
+    for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) rc = set_partition_stream(s, s->lanes[l].ctx, (int)l, hi);
+    for (uint32_t i = 0; rc == BBTC_OK && i < s->load_ctx.size(); i++)
+      rc = set_partition_stream(s, s->load_ctx[i], (int)(i % 2), i % 2 == 0 ? mid : lo);
   }
   for (uint32_t l = 0; rc == BBTC_OK && l < 2; l++) {
     if (dev_malloc_sync(&s->lanes[l].d_outs, s->opts.max_batch * sizeof(uint64_t)) != cudaSuccess ||
@@ -370,6 +459,8 @@ int bbtc_server_create(int device, const bbtc_server_opts* opts, bbtc_server** o
       if (L.d_outs) cudaFree(L.d_outs);
       if (L.h_outs) cudaFreeHost(L.h_outs);
     }
+    for (CUgreenCtx g : s->green)
+      if (g) green_api().destroy(g);
     delete s;
     return rc;
   }
@@ -450,6 +541,8 @@ int bbtc_server_destroy(bbtc_server* s) {
   }
   for (auto* c : s->load_ctx) bbtc_ctx_destroy(c);
   for (auto& L : s->lanes) bbtc_ctx_destroy(L.ctx);
+  for (CUgreenCtx g : s->green)  // after the streams in them are destroyed
+    if (g) green_api().destroy(g);
   {
     // hand the pool's unused memory back (it was grown to the budget at creation)
     cudaMemPool_t pool;

@@ -89,6 +89,13 @@ def parse():
                    help="serve: small requests go through the copy engines even from page-locked buffers")
     p.add_argument("--trace", default="", help="serve: write every request's stage timestamps to this JSON file")
     p.add_argument("--rates", default="", help="serve: comma-separated rates, one stream each on one server")
+    p.add_argument("--large-bps", type=int, default=0, help="serve: persistent blocks per SM of the large lane (0: 3)")
+    p.add_argument("--large-layout-bps", type=int, default=0,
+                   help="serve: layout blocks per SM of large requests (0: 2)")
+    p.add_argument("--small-sms", type=int, default=-1,
+                   help="serve: SMs of the small requests' partition (0: none; -1: the server's default)")
+    p.add_argument("--max-large-loads", type=int, default=-1,
+                   help="serve: large requests loading at once (0: no limit; -1: the server's default)")
     p.add_argument("--no-check", action="store_true", help="batch / serve: skip the oracle counts")
     p.add_argument("--no-batch", action="store_true", help="default line: no batched-launch sub-record")
     p.add_argument("--no-serve", action="store_true", help="default line: no serving sub-record")
@@ -492,7 +499,8 @@ def serve_once(srv, pool, max_scale: int, rate: float, duration: float, seed: in
 
 
 def measure_serve(max_scale: int, rates, duration: float, loaders: int, pin: bool, copy_engine_uploads: bool,
-                  check: bool = True, trace=None) -> dict:
+                  check: bool = True, trace=None, large_bps: int = 0, large_layout_bps: int = 0,
+                  max_large_loads: int = -1, small_sms: int = -1) -> dict:
     """Pool generation, oracle counts of every pool graph, one warm-up
     request per scale, then one Poisson stream per rate on the same server."""
     from bbtc_b200 import Server
@@ -506,7 +514,10 @@ def measure_serve(max_scale: int, rates, duration: float, loaders: int, pin: boo
         keys = [(s, j) for s in sorted(pool) for j in range(len(pool[s]))]
         want = dict(zip(keys, oracle_counts(items)))
     oracle_s = time.time() - t0
-    srv = Server(0, loaders=loaders, copy_engine_uploads=copy_engine_uploads)
+    srv = Server(0, loaders=loaders, copy_engine_uploads=copy_engine_uploads, large_blocks_per_sm=large_bps,
+                 large_layout_blocks_per_sm=large_layout_bps,
+                 max_large_loads=None if max_large_loads < 0 else max_large_loads,
+                 small_sms=None if small_sms < 0 else small_sms)
     try:
         for s in sorted(pool):
             g, c = pool[s][0]
@@ -520,7 +531,8 @@ def measure_serve(max_scale: int, rates, duration: float, loaders: int, pin: boo
     del keep
     return {"runs": runs, "pool_graphs": sum(len(v) for v in pool.values()), "generate_s": round(gen_s, 1),
             "oracle_s": round(oracle_s, 1), "launches": st.launches, "max_batch": st.max_batch,
-            "loaders": loaders, "pinned_requests": pin,
+            "loaders": loaders, "pinned_requests": pin, "large_blocks_per_sm": large_bps or 3,
+            "large_layout_blocks_per_sm": large_layout_bps or 2, "small_sms": small_sms,
             "small_uploads": "copy engines" if copy_engine_uploads or not pin else "kernel reads",
             "workload": f"serving: Poisson arrivals, R-MAT scale 12+Geom(0.3) <= {max_scale}, ef 16"}
 
@@ -529,7 +541,9 @@ def run_serve(args):
     rates = [float(x) for x in args.rates.split(",")] if args.rates else [args.rate]
     trace = [] if args.trace else None
     sv = measure_serve(args.serve_max_scale, rates, args.duration, args.loaders, bool(args.pin),
-                       args.copy_engine_uploads, check=not args.no_check, trace=trace)
+                       args.copy_engine_uploads, check=not args.no_check, trace=trace, large_bps=args.large_bps,
+                       large_layout_bps=args.large_layout_bps, max_large_loads=args.max_large_loads,
+                       small_sms=args.small_sms)
     if args.trace:
         with open(args.trace, "w") as f:
             json.dump({"fields": ["scale", "m", "submit_ns", "load_ns", "ready_ns", "launch_ns", "done_ns", "batch"],

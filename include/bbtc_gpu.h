@@ -180,7 +180,7 @@ typedef struct bbtc_opts {
   uint32_t blocks_per_sm;    /* persistent grid = SMs x this, 0 = occupancy limit */
   int use_cuda_graph;        /* replay the launch sequence through a captured CUDA graph */
   int sort_tasks;            /* when tasks == NULL: 1 = cost-sorted descending (default) */
-  uint32_t occupancy;        /* persistent form: register budget for 4, 6 or 8 blocks per SM (0: 6 for
+  uint32_t occupancy;        /* persistent form: register budget for 4, 5, 6 or 8 blocks per SM (5: fused task rows only; 0: 6 for
                                 fused task rows with a bitmap of at most 1024 words, else 4) */
 } bbtc_opts;
 
@@ -291,6 +291,13 @@ typedef struct bbtc_server_opts {
   uint32_t aging_ms;      /* a request waiting this long is loaded before smaller ones (default 50) */
   uint64_t pool_bytes;    /* the device memory pool is grown to this size at creation, so loads never
                              wait for it to grow (0 = 1.1 x hbm_budget; at most the free memory less 8 GiB) */
+  uint32_t large_layout_blocks_per_sm; /* grid cap of the large requests' layout kernels, blocks of 256 threads per
+                                          SM (0 = 2), so that small requests' kernels find room on every SM */
+  uint32_t max_large_loads; /* large requests uploaded and laid out at once, at most (0 = no limit) */
+  uint32_t small_sms;       /* > 0: a partition of this many SMs (a multiple of 8; green contexts) runs the small
+                               requests' loads and counts, the other SMs the large ones', so neither waits for
+                               the other's blocks (0 = all SMs shared) */
+  uint32_t reserved;
 } bbtc_server_opts;
 typedef struct bbtc_request_info {
   uint64_t count;     /* exact count once status == 1 */

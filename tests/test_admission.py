@@ -15,10 +15,12 @@ PROGRAM = r"""
 #include <vector>
 #include "admission.hpp"
 struct R { uint64_t m, reserved, t_submit; };
-static long pick(std::vector<R>& rs, uint64_t budget, uint64_t in_use, uint64_t now, bool small_only) {
+static long pick(std::vector<R>& rs, uint64_t budget, uint64_t in_use, uint64_t now, bool small_only,
+                 bool large_ok = true) {
   std::vector<const R*> p;
   for (auto& r : rs) p.push_back(&r);
-  const bbtc::AdmitLimits lim{budget, in_use, /*small_edges=*/1000, /*aging_ns=*/50, now, small_only, 4096};
+  bbtc::AdmitLimits lim{budget, in_use, /*small_edges=*/1000, /*aging_ns=*/50, now, small_only, 4096};
+  lim.large_ok = large_ok;
   const size_t i = bbtc::admit_pick(p, lim);
   return i == SIZE_MAX ? -1 : (long)i;
 }
@@ -34,6 +36,9 @@ int main() {
   std::vector<R> d{{5000, 10, 0}, {4000, 10, 1}};
   std::printf("small_only %ld\n", pick(d, 1000, 0, 10, true));       // -1: both are large
   std::printf("any_loader %ld\n", pick(d, 1000, 0, 10, false));      // 1
+  std::printf("large_busy %ld\n", pick(d, 1000, 0, 60, false, false)); // -1: large loads at their limit, even aged
+  std::vector<R> f{{5000, 10, 0}, {40, 10, 1}};
+  std::printf("small_while_large %ld\n", pick(f, 1000, 0, 60, false, false)); // 1
   std::vector<R> e;
   std::printf("none %ld\n", pick(e, 1000, 0, 10, false));            // -1
   return 0;
@@ -53,4 +58,5 @@ def test_admission_policy(tmp_path):
     out = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True,
                                                  text=True).stdout.splitlines())
     assert out == {"smallest": "1", "aged": "0", "budget": "1", "empty_device": "0", "never_fits": "0",
-                   "small_only": "-1", "any_loader": "1", "none": "-1"}
+                   "small_only": "-1", "any_loader": "1", "none": "-1", "large_busy": "-1",
+                   "small_while_large": "1"}

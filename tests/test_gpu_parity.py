@@ -465,3 +465,20 @@ def test_unoriented_wide_pivots(ctx, bitmap_words):
                 assert got == want, (P, kernel, mode, bitmap_words)
         finally:
             st.free()
+
+
+def test_batch_configuration_draw_against_oracle(ctx):
+    """The batched-launch configuration's generator mix, down-scaled (512
+    R-MAT graphs of scale 10-12, edge factor 8-32, and 64 random geometric
+    graphs of 2^14-2^18 points, each with its own uni ncut 4-16): one
+    persistent launch counts every graph as the oracle does."""
+    import bench
+    work = bench.batch_workload(12)
+    assert len(work) == 576
+    want = bench.oracle_counts(work)
+    sts = [Graph.from_csr(ctx, g, c) for g, c in work]
+    try:
+        assert count_batch(ctx, sts) == want
+    finally:
+        for st in sts:
+            st.free()

@@ -128,3 +128,24 @@ def test_pinned_requests_counted_right():
                 info = srv.wait(rid, 60000)
                 assert info.status == 1 and info.count == want[i], (gs[i].name, info.status, info.count, want[i])
                 srv.release(rid)
+
+
+@pytest.mark.parametrize("small_sms", [8, 24])
+def test_partitioned_server_counts(small_sms):
+    """Small and large requests on separate SM partitions (green contexts):
+    every count equals the oracle's, requests of both classes in flight at
+    once, and a partition that leaves no SMs for the large requests is
+    refused."""
+    gs = mix() + [graphs.rmat(17, 16, seed=41)]
+    small_edges = 1 << 16  # the s17 graph and the larger mix graphs take the large partition
+    cuts = [graphs.cuts(g, 4 + i % 3, "uni") for i, g in enumerate(gs)]
+    want = [oracle.count(g.n, g.indptr, g.indices, c) for g, c in zip(gs, cuts)]
+    assert any(g.m > small_edges for g in gs) and any(g.m <= small_edges for g in gs)
+    with Server(0, loaders=2, small_edges=small_edges, small_sms=small_sms) as srv:
+        ids = [(srv.submit_csr(g, c), i) for _ in range(3) for i, (g, c) in enumerate(zip(gs, cuts))]
+        for rid, i in ids:
+            info = srv.wait(rid, 60000)
+            assert info.status == 1 and info.count == want[i], (gs[i].name, info.status, info.count, want[i])
+            srv.release(rid)
+    with pytest.raises(BBTcError):
+        Server(0, small_sms=100000)
