@@ -45,9 +45,11 @@ sys.path.insert(0, ROOT)
 METRIC = "edges/sec at exact count, batched vs plain form on 1 B200; p50/p99 latency"
 UNIT = "edges/s"
 FALLBACK_HBM_GBS = 6650.0
-# serving throughput peak on one B200 (requests/s at which edges/s stopped
-# growing in a rate sweep); the default line serves at 80 % of it
-SERVE_PEAK_RPS = 1000.0
+# serving throughput peak on one B200: requests/s served when the offered
+# rate exceeds what the server sustains (1,800 req/s offered: 1,508-1,527
+# served, 4.58e9-4.68e9 edges/s, three runs); the default line serves at 80 %
+# of it
+SERVE_PEAK_RPS = 1510.0
 
 
 def parse():
@@ -653,12 +655,9 @@ def main():
     t_max = t_mean
     m_total = g.m
     if dist is not None:
-        tt = torch.tensor([t_mean], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        mm = torch.tensor([g.m, count], dtype=torch.int64, device=f"cuda:{local}")
-        dist.all_reduce(mm)
-        m_total, count_total = int(mm[0].item()), int(mm[1].item())
+        # the only exchange: edges and counts summed, the slowest rank's time
+        from bbtc_b200 import multi
+        m_total, count_total, t_max = multi.aggregate(dist, g.m, count, t_mean, device=f"cuda:{local}")
     value = m_total / t_max
 
     # --- plain form (one launch per task) ---
