@@ -845,13 +845,18 @@ __device__ __forceinline__ void fused_build_words(const uint2* __restrict__ pw, 
 __device__ __forceinline__ void fused_build_rank(const uint2* __restrict__ pw, uint32_t wn, uint32_t mask0,
                                                  uint32_t fw, uint32_t blocks, uint32_t* bm, uint32_t lane) {
   uint32_t* masks = bm + 2 * blocks;
-  for (uint32_t i = lane; i < wn; i += 32) {
-    const uint2 w = pw[i];
-    const uint32_t rel = w.x - fw;
-    const uint32_t blk = rel >> 5;
-    atomicOr(&bm[2 * blk], 1u << (rel & 31));
-    if (i == 0 || ((pw[i - 1].x - fw) >> 5) != blk) bm[2 * blk + 1] = i;
-    masks[i] = i == 0 ? (w.y & mask0) : w.y;
+  for (uint32_t c = 0; c < wn; c += 32) {  // every lane runs every round: the shuffle needs them all
+    const uint32_t i = c + lane;
+    const uint2 w = i < wn ? pw[i] : make_uint2(fw, 0u);
+    uint32_t prev = __shfl_up_sync(FULL, w.x, 1);  // the previous pair's word, from the lane before
+    if (lane == 0 && c > 0) prev = pw[c - 1].x;
+    if (i < wn) {
+      const uint32_t rel = w.x - fw;
+      const uint32_t blk = rel >> 5;
+      atomicOr(&bm[2 * blk], 1u << (rel & 31));
+      if (i == 0 || ((prev - fw) >> 5) != blk) bm[2 * blk + 1] = i;
+      masks[i] = i == 0 ? (w.y & mask0) : w.y;
+    }
   }
 }
 
