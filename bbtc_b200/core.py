@@ -383,7 +383,7 @@ class ServerOpts(c.Structure):
                 ("loaders", c.c_uint32), ("copy_engine_uploads", c.c_uint32), ("count", Opts),
                 ("small_edges", c.c_uint64), ("large_blocks_per_sm", c.c_uint32), ("aging_ms", c.c_uint32),
                 ("pool_bytes", c.c_uint64), ("large_layout_blocks_per_sm", c.c_uint32),
-                ("max_large_loads", c.c_uint32), ("small_sms", c.c_uint32), ("reserved", c.c_uint32)]
+                ("max_large_loads", c.c_uint32), ("small_sms", c.c_uint32), ("small_aging_us", c.c_uint32)]
 
 
 class RequestInfo(c.Structure):
@@ -427,7 +427,8 @@ class Server:
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch: int = 0, loaders: int = 0,
                  opts: Opts | None = None, small_edges: int = 0, large_blocks_per_sm: int = 0,
                  aging_ms: int | None = None, pool_bytes: int = 0, copy_engine_uploads: bool = False,
-                 large_layout_blocks_per_sm: int = 0, max_large_loads: int | None = None, small_sms: int | None = None):
+                 large_layout_blocks_per_sm: int = 0, max_large_loads: int | None = None, small_sms: int | None = None,
+                 small_aging_us: int | None = None):
         L = _server_lib()
         so = ServerOpts()
         L.bbtc_server_opts_default(c.byref(so))
@@ -453,6 +454,8 @@ class Server:
             so.max_large_loads = max_large_loads
         if small_sms is not None:
             so.small_sms = small_sms
+        if small_aging_us is not None:
+            so.small_aging_us = small_aging_us
         so.copy_engine_uploads = 1 if copy_engine_uploads else 0
         self._h = c.c_void_p()
         check(L.bbtc_server_create(device, c.byref(so), c.byref(self._h)))

@@ -3,9 +3,11 @@
 //
 // A loader takes, among the pending requests that the HBM budget admits (or
 // that can never fit, so that they fail at once), the oldest one that has
-// waited `aging_ns` or more, else the one with the fewest edges: small
-// requests overtake large loads, and large ones are not starved.  A loader
-// reserved for small requests sees only those.  No counterpart in the
+// waited its class's aging time or more (`small_aging_ns` for small requests,
+// `aging_ns` for large ones), else the one with the fewest edges: small
+// requests overtake large loads, large ones are not starved, and a small
+// request is not passed over by smaller ones for longer than its aging time.
+// A loader reserved for small requests sees only those.  No counterpart in the
 // reference, which counts one graph per process.
 #pragma once
 #include <cstddef>
@@ -22,6 +24,7 @@ struct AdmitLimits {
   bool small_only;       // the loader takes small requests only
   size_t scan_limit;     // pending requests looked at
   bool large_ok = true;  // false: as many large requests are loading as the server allows at once
+  uint64_t small_aging_ns = 0;  // a small request waiting this long is taken before smaller ones (0: aging_ns)
 };
 
 // Index in `pending` (a random-access sequence of pointers to objects with
@@ -36,7 +39,8 @@ size_t admit_pick(const Seq& pending, const AdmitLimits& lim) {
     if ((lim.small_only || !lim.large_ok) && r->m > lim.small_edges) continue;
     const bool never = r->reserved > lim.budget;
     if (!never && lim.in_use + r->reserved > lim.budget && lim.in_use != 0) continue;
-    if (lim.now_ns - r->t_submit >= lim.aging_ns) return i;
+    const uint64_t aging = r->m <= lim.small_edges && lim.small_aging_ns ? lim.small_aging_ns : lim.aging_ns;
+    if (lim.now_ns - r->t_submit >= aging) return i;
     if (best == SIZE_MAX || r->m < pending[best]->m) best = i;
   }
   return best;

@@ -210,9 +210,12 @@ int bbtc_ctx_create(int device, bbtc_ctx** out) {
 int bbtc_ctx_destroy(bbtc_ctx* ctx) {
   if (!ctx) return BBTC_OK;
   cudaSetDevice(ctx->device);
+  if (ctx->d_scratch) cudaFreeAsync(ctx->d_scratch, ctx->stream);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->d_unit_counter) cudaFree(ctx->d_unit_counter);
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+  if (ctx->h_plan_done) cudaEventDestroy(ctx->h_plan_done);
+  if (ctx->h_plan) cudaFreeHost(ctx->h_plan);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return BBTC_OK;

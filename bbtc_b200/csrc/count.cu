@@ -1236,14 +1236,6 @@ void Plan::release() {
   d_tasks = nullptr;
   d_prefix = nullptr;
   cap = 0;
-  if (h_done) {
-    cudaEventSynchronize(h_done);  // no upload still reads h_buf
-    cudaEventDestroy(h_done);
-    h_done = nullptr;
-  }
-  if (h_buf) cudaFreeHost(h_buf);
-  h_buf = nullptr;
-  h_cap = 0;
 }
 
 static int enqueue_launches(bbtc_ctx* ctx, Plan* plan, const bbtc_opts& o, uint64_t* d_outs, uint32_t nouts) {
@@ -1345,24 +1337,26 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
         }
         plan->cap = cap;
       }
-      // upload from pinned staging (a pageable copy would go through the
-      // driver's shared staging buffers, which other threads' copies hold)
+      // upload from the context's pinned staging (a pageable copy would go
+      // through the driver's shared staging buffers, which other threads'
+      // copies hold); the context keeps it across plans, since pinning host
+      // memory can take milliseconds
       const size_t tb = nt * sizeof(DevTask), pb = (nt + 1) * sizeof(uint32_t);
-      if (plan->h_done) BBTC_CUDA(cudaEventSynchronize(plan->h_done));  // the last upload has read h_buf
-      if (tb + pb > plan->h_cap) {
-        if (plan->h_buf) cudaFreeHost(plan->h_buf);
-        plan->h_buf = nullptr;
-        plan->h_cap = 0;
+      if (ctx->h_plan_done) BBTC_CUDA(cudaEventSynchronize(ctx->h_plan_done));  // the last upload has read it
+      if (tb + pb > ctx->h_plan_cap) {
+        if (ctx->h_plan) cudaFreeHost(ctx->h_plan);
+        ctx->h_plan = nullptr;
+        ctx->h_plan_cap = 0;
         const size_t want = std::max<size_t>(tb + pb, 64 << 10) * 2;
-        BBTC_CUDA(cudaMallocHost(&plan->h_buf, want));
-        plan->h_cap = want;
+        BBTC_CUDA(cudaMallocHost(&ctx->h_plan, want));
+        ctx->h_plan_cap = want;
       }
-      if (!plan->h_done) BBTC_CUDA(cudaEventCreateWithFlags(&plan->h_done, cudaEventDisableTiming));
-      std::memcpy(plan->h_buf, plan->tasks.data(), tb);
-      std::memcpy(plan->h_buf + tb, plan->prefix.data(), pb);
-      BBTC_CUDA(cudaMemcpyAsync(plan->d_tasks, plan->h_buf, tb, cudaMemcpyHostToDevice, s));
-      BBTC_CUDA(cudaMemcpyAsync(plan->d_prefix, plan->h_buf + tb, pb, cudaMemcpyHostToDevice, s));
-      BBTC_CUDA(cudaEventRecord(plan->h_done, s));
+      if (!ctx->h_plan_done) BBTC_CUDA(cudaEventCreateWithFlags(&ctx->h_plan_done, cudaEventDisableTiming));
+      std::memcpy(ctx->h_plan, plan->tasks.data(), tb);
+      std::memcpy(ctx->h_plan + tb, plan->prefix.data(), pb);
+      BBTC_CUDA(cudaMemcpyAsync(plan->d_tasks, ctx->h_plan, tb, cudaMemcpyHostToDevice, s));
+      BBTC_CUDA(cudaMemcpyAsync(plan->d_prefix, ctx->h_plan + tb, pb, cudaMemcpyHostToDevice, s));
+      BBTC_CUDA(cudaEventRecord(ctx->h_plan_done, s));
     }
     plan->captured = false;
   }
@@ -1372,7 +1366,10 @@ int count_enqueue(bbtc_ctx* ctx, const std::vector<bbtc_graph*>& graphs,
     plan->captured = false;
   }
   plan->stage_polls = ctx->debug_stage_polls;
-  if (!o.use_cuda_graph) return enqueue_launches(ctx, plan, o, d_outs, (uint32_t)graphs.size());
+  // A plan's first count launches directly: capturing and instantiating a
+  // graph costs more host time than one launch, and pays only on replays,
+  // so the capture waits for the plan's second count.
+  if (!o.use_cuda_graph || !reuse) return enqueue_launches(ctx, plan, o, d_outs, (uint32_t)graphs.size());
   if (!plan->captured) {
     cudaGraph_t graph = nullptr;
     BBTC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));

@@ -139,9 +139,6 @@ struct Plan {
   uint32_t total_units = 0;
   uint32_t launches = 0;
   bool fused = false;              // every task is a fused task row
-  char* h_buf = nullptr;           // pinned staging of the task queue's upload
-  size_t h_cap = 0;
-  cudaEvent_t h_done = nullptr;    // recorded after the last upload from h_buf
   cudaGraphExec_t exec = nullptr;
   bool captured = false;
   uint32_t stage_polls = 0;        // the context's staging test hook when the launch was captured
@@ -169,19 +166,40 @@ struct bbtc_ctx {
   // waited for a long kernel on its stream held up the copies of all other
   // threads; copies from pinned memory wait only for their own stream.
   char* h_stage = nullptr;
+  // Pinned staging of the task queues' uploads, kept across plans.
+  char* h_plan = nullptr;
+  size_t h_plan_cap = 0;
+  cudaEvent_t h_plan_done = nullptr;  // recorded after the last upload from h_plan
+  // Layout scratch kept between builds (bbtc::Scratch), at most kScratchKeep bytes.
+  char* d_scratch = nullptr;
+  size_t scratch_cap = 0;
 };
 
 namespace bbtc {
 
-// Stream-ordered device buffer (freed on the stream it was allocated on).
+// Scratch of one layout build: its temporaries are carved from one device
+// block that the context keeps between builds, so a build whose temporaries
+// fit makes no allocation call for them.  `want` sums what the build asked
+// for (256-byte rounded), carved or not; the block grows to it afterwards.
+struct Scratch {
+  char* base = nullptr;
+  size_t cap = 0, off = 0, want = 0;
+};
+// The build running on this thread, if any (one build at a time per context,
+// and a context's builds run on the thread that called them).
+inline thread_local Scratch* t_scratch = nullptr;
+
+// Stream-ordered device buffer (freed on the stream it was allocated on);
+// carved from the running build's scratch when that has room.
 struct DevBuf {
   void* p = nullptr;
   cudaStream_t s = nullptr;
+  bool carved = false;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() {
-    if (p) cudaFreeAsync(p, s);
+    if (p && !carved) cudaFreeAsync(p, s);
   }
   template <class T>
   T* as() { return static_cast<T*>(p); }
@@ -189,6 +207,16 @@ struct DevBuf {
 
 inline int dalloc(DevBuf& b, size_t bytes, cudaStream_t s) {
   b.s = s;
+  if (Scratch* a = t_scratch) {
+    const size_t need = ((bytes > 16 ? bytes : 16) + 255) & ~static_cast<size_t>(255);
+    a->want += need;
+    if (a->off + need <= a->cap) {
+      b.p = a->base + a->off;
+      b.carved = true;
+      a->off += need;
+      return BBTC_OK;
+    }
+  }
   cudaError_t e = dev_malloc(&b.p, bytes > 16 ? bytes : 16, s);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -201,7 +229,7 @@ inline int dalloc(DevBuf& b, size_t bytes, cudaStream_t s) {
 
 // Regions of bbtc_ctx::h_stage (one graph build or count at a time per context).
 constexpr size_t kStageBytes = 1u << 20;
-constexpr size_t kStageCuts = 0;          // cut vector, <= (64 + 1) x 4 bytes
+constexpr size_t kStageCuts = 0;          // cut vector and a flags word, <= (64 + 2) x 4 bytes
 constexpr size_t kStageBad = 3072;        // validation flags
 constexpr size_t kStageOff[2] = {4096, 40960};  // per block CSR: tile + part row offsets (<= 33,288 bytes)
 constexpr size_t kStageStats = 81920;     // tile statistics of both block CSRs (<= 163,840 bytes)

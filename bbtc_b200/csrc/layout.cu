@@ -65,10 +65,10 @@ __device__ __forceinline__ uint32_t lower_bound_range(const uint32_t* __restrict
 // Host-to-device copy done by the SMs: `src` is page-locked host memory
 // mapped into the device's address space, read over the host link, so the
 // copy does not queue behind other streams' transfers on the copy engines.
-// `dst` is a device allocation (256-byte aligned); words = bytes / 4.
-__global__ void k_copy_mapped(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint64_t words) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// Each `dst` is a device allocation (256-byte aligned); words = bytes / 4.
+// Two arrays per launch (a graph's row pointers and ids); words1 may be 0.
+__device__ __forceinline__ void copy_words(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                           uint64_t words, uint64_t t0, uint64_t stride) {
   uint64_t done = 0;
   if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
     const uint64_t v = words / 4;
@@ -80,30 +80,39 @@ __global__ void k_copy_mapped(uint32_t* __restrict__ dst, const uint32_t* __rest
   for (uint64_t i = done + t0; i < words; i += stride) dst[i] = src[i];
 }
 
-// Input contract check: monotone row pointers, strictly increasing rows, ids < n.
-__global__ void k_validate_rows(const uint32_t* __restrict__ indptr, uint32_t n, uint64_t m,
-                                uint32_t* __restrict__ bad) {
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
-    if (u == 0 && indptr[0] != 0) atomicOr(bad, 1u);
-    if (u == n - 1 && (uint64_t)indptr[n] != m) atomicOr(bad, 2u);
-    if (indptr[u + 1] < indptr[u] || (uint64_t)indptr[u + 1] > m) atomicOr(bad, 4u);
-  }
+__global__ void k_copy_mapped(uint32_t* __restrict__ dst0, const uint32_t* __restrict__ src0, uint64_t words0,
+                              uint32_t* __restrict__ dst1, const uint32_t* __restrict__ src1, uint64_t words1) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  copy_words(dst0, src0, words0, t0, stride);
+  copy_words(dst1, src1, words1, t0, stride);
 }
 
-// Expands the row id of every edge and checks ids; rows whose pointers are
-// out of order or past m are skipped (k_validate_rows flags them).  With
-// `flags`, also marks the edges that open a new 32-id word of their row
-// (flags[e] = 1), the input of the word-compressed rows.
+// Input contract check and per-edge expansion, one warp per row: row
+// pointers start at 0, never decrease and end at m; rows are strictly
+// increasing; ids are < n.  Rows whose pointers are out of order or past m
+// are flagged and skipped.  Writes the row id of every edge; with `flags`,
+// marks the edges that open a new 32-id word of their row (flags[e] = 1), the
+// input of the word-compressed rows; with `iota`, iota[e] = e (the edge ids
+// that the reversed graph's sort carries).  Nothing downstream reads `bad`
+// on the host before the layout is done: every later kernel that indexes by
+// these arrays returns at once when `*bad` is set.
 __global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
                                uint32_t n, uint64_t m, uint32_t* __restrict__ rows, uint32_t* __restrict__ bad,
-                               uint32_t* __restrict__ flags) {
+                               uint32_t* __restrict__ flags, uint32_t* __restrict__ iota) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = warp; u < n; u += nwarps) {
     const uint32_t a = indptr[u], b = indptr[u + 1];
-    if (b < a || (uint64_t)b > m) continue;
+    if (lane == 0) {
+      if (u == 0 && a != 0) atomicOr(bad, 1u);
+      if (u == n - 1 && (uint64_t)b != m) atomicOr(bad, 2u);
+    }
+    if (b < a || (uint64_t)b > m) {
+      if (lane == 0) atomicOr(bad, 4u);
+      continue;
+    }
     for (uint32_t e = a + lane; e < b; e += 32) {
       rows[e] = u;
       const uint32_t c = indices[e];
@@ -111,6 +120,7 @@ __global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32
       if (c >= n) atomicOr(bad, 8u);
       if (e > a && prev >= c) atomicOr(bad, 16u);
       if (flags) flags[e] = (e == a || (c >> 5) != (prev >> 5)) ? 1u : 0u;
+      if (iota) iota[e] = e;
     }
   }
 }
@@ -122,7 +132,8 @@ __global__ void k_expand_check(const uint32_t* __restrict__ indptr, const uint32
 __global__ void k_entry_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
                               const uint32_t* __restrict__ rows, uint64_t m, const uint32_t* __restrict__ cuts_g,
                               uint32_t P, const uint64_t* __restrict__ rp_off, uint32_t* __restrict__ counts,
-                              uint32_t* __restrict__ runs) {
+                              uint32_t* __restrict__ runs, const uint32_t* __restrict__ bad) {
+  if (*bad) return;
   __shared__ uint32_t cuts[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
   __syncthreads();
@@ -141,39 +152,37 @@ __global__ void k_entry_count(const uint32_t* __restrict__ indptr, const uint32_
   }
 }
 
-// base[t] = value of the scanned pool at tile t's first slot (sum of all earlier counts).
-__global__ void k_tile_base(const uint32_t* __restrict__ rp, const uint64_t* __restrict__ rp_off, uint32_t T,
-                            uint32_t* __restrict__ base) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
-    base[t] = rp[rp_off[t]];
-}
+// Up to four zero fills of layout buffers in one launch, on the SMs (at the
+// stream's priority, leaving the copy engines to the uploads); each range
+// starts on a 16-byte boundary.
+struct ZeroRanges {
+  uint32_t* p[4];
+  uint64_t words[4];
+};
 
-// Zero fill of the large layout buffers on the SMs (a grid-stride kernel at
-// the stream's priority), leaving the copy engines to the uploads.
-__global__ void k_zero(uint32_t* __restrict__ p, uint64_t nwords) {
-  uint4* __restrict__ q = reinterpret_cast<uint4*>(p);
-  const uint64_t n4 = nwords / 4;
+__global__ void k_zero_ranges(ZeroRanges z) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (uint64_t i = t0; i < n4; i += stride) q[i] = make_uint4(0, 0, 0, 0);
-  for (uint64_t i = n4 * 4 + t0; i < nwords; i += stride) p[i] = 0;
+  for (int r = 0; r < 4; r++) {
+    uint32_t* __restrict__ p = z.p[r];
+    const uint64_t nwords = z.words[r];
+    uint4* __restrict__ q = reinterpret_cast<uint4*>(p);
+    const uint64_t n4 = nwords / 4;
+    for (uint64_t i = t0; i < n4; i += stride) q[i] = make_uint4(0, 0, 0, 0);
+    for (uint64_t i = n4 * 4 + t0; i < nwords; i += stride) p[i] = 0;
+  }
 }
 
-int zero_fill(void* p, uint64_t bytes, cudaStream_t s, int grid) {
-  k_zero<<<grid, 256, 0, s>>>(static_cast<uint32_t*>(p), bytes / 4);  // callers pass multiples of 4 bytes
-  BBTC_CUDA(cudaGetLastError());
-  return BBTC_OK;
-}
-
-// One pass over the row-pointer pool: subtract each tile's base from its
-// slots (row pointers become tile-local), and per tile the longest row and
-// the number of non-empty rows.  A row's length is its run count (the scan
-// input), so the pass reads no neighbouring slot that another thread is
-// rewriting; lanes of one tile are combined before the atomics.
-__global__ void k_localize_stats(uint32_t* __restrict__ rp, const uint32_t* __restrict__ counts,
+// One pass over the row-pointer pool: `scanned` is the inclusive scan of the
+// run counts, so a slot minus its tile's first slot is the tile-local row
+// pointer written to `rp`; per tile, the longest row and the number of
+// non-empty rows (a row's length is the difference of two scanned slots).
+// Lanes of one tile are combined before the atomics.
+__global__ void k_localize_stats(uint32_t* __restrict__ rp, const uint32_t* __restrict__ scanned,
                                  const uint32_t* __restrict__ cuts_g, uint32_t P,
-                                 const uint64_t* __restrict__ part_off, const uint32_t* __restrict__ base,
-                                 uint64_t len, uint32_t* __restrict__ maxdeg, uint32_t* __restrict__ nerows) {
+                                 const uint64_t* __restrict__ part_off, uint64_t len, uint32_t* __restrict__ maxdeg,
+                                 uint32_t* __restrict__ nerows, const uint32_t* __restrict__ bad) {
+  if (*bad) return;
   __shared__ uint32_t cuts[kMaxParts + 1];
   __shared__ uint64_t poff[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) {
@@ -197,9 +206,10 @@ __global__ void k_localize_stats(uint32_t* __restrict__ rp, const uint32_t* __re
       const uint64_t A = (poff[lo + 1] - poff[lo]) / P;  // slots per tile of this row part
       const uint32_t y = (uint32_t)((s - poff[lo]) / A);
       const uint32_t r = (uint32_t)(s - poff[lo] - (uint64_t)y * A);
-      rp[s] -= base[lo * P + y];
+      const uint32_t v = scanned[s];
+      rp[s] = v - scanned[poff[lo] + (uint64_t)y * A];
       if (r < cuts[lo + 1] - cuts[lo]) {
-        rowlen = counts[s + 1];  // rp[s + 1] - rp[s] before or after the rebase
+        rowlen = scanned[s + 1] - v;
         tile = lo * P + y;
       }
     }
@@ -216,8 +226,8 @@ __global__ void k_localize_stats(uint32_t* __restrict__ rp, const uint32_t* __re
 // nnz per tile and 16-byte aligned column offsets of the non-empty tiles (one block).
 __global__ void k_tile_offsets(const uint32_t* __restrict__ rp, const uint64_t* __restrict__ rp_off,
                                const uint32_t* __restrict__ cuts, uint32_t P, uint32_t* __restrict__ nnz,
-                               uint64_t* __restrict__ col_off) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+                               uint64_t* __restrict__ col_off, const uint32_t* __restrict__ bad) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || *bad) return;
   uint64_t cur = 0;
   for (uint32_t t = 0; t < P * P; t++) {
     const uint32_t x = t / P;
@@ -234,9 +244,9 @@ __global__ void k_tile_offsets(const uint32_t* __restrict__ rp, const uint64_t* 
 // exactly one non-empty row, so each slot has one writer.  blockIdx.y = tile.
 __global__ void k_row_index(const uint32_t* __restrict__ rp, const uint64_t* __restrict__ rp_off,
                             const uint32_t* __restrict__ cuts, uint32_t P, const uint64_t* __restrict__ col_off,
-                            uint32_t* __restrict__ erow) {
+                            uint32_t* __restrict__ erow, const uint32_t* __restrict__ bad) {
   const uint32_t t = blockIdx.y;
-  if (col_off[t] == kNoSegment) return;
+  if (*bad || col_off[t] == kNoSegment) return;
   const uint32_t x = t / P;
   const uint32_t H = cuts[x + 1] - cuts[x];
   const uint32_t* __restrict__ r = rp + rp_off[t];
@@ -290,7 +300,8 @@ __global__ void k_entry_scatter(const uint32_t* __restrict__ runs, const uint32_
                                 const uint32_t* __restrict__ eids, const uint32_t* __restrict__ wpos,
                                 const uint32_t* __restrict__ wptr, uint2* __restrict__ rec,
                                 const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fidx,
-                                const uint2* __restrict__ words) {
+                                const uint2* __restrict__ words, const uint32_t* __restrict__ bad) {
+  if (*bad) return;
   __shared__ uint32_t cuts[kMaxParts + 1];
   for (uint32_t t = threadIdx.x; t <= P; t += blockDim.x) cuts[t] = cuts_g[t];
   __syncthreads();
@@ -316,23 +327,52 @@ __global__ void k_entry_scatter(const uint32_t* __restrict__ runs, const uint32_
 // Word-compressed rows: each row's ids grouped by 32-id word into (word, bit
 // mask) pairs.  flags[e] = 1 when edge e opens a new word of its row
 // (k_expand_check); wpos = their inclusive scan, so edge e lands in pair
-// wpos[e] - 1.
+// wpos[e] - 1.  A warp takes 32 consecutive edges; a pair's edges are
+// consecutive, so a segmented suffix OR by shuffles (five steps, no
+// divergence) gives the first lane of each pair in the chunk the bits of the
+// pair's edges in the chunk.  The lane of the edge that opens a pair stores
+// it, after ORing in the bits of its edges past the chunk (at most 31 more,
+// only for the chunk's last pair); a pair that opened in an earlier chunk is
+// that chunk's to store.  So each pair has one writer and no atomics.  Pairs
+// W = wpos[m - 1] .. m + 1 (the array's unused tail) are zeroed.  Needs m > 0.
 __global__ void k_word_fill(const uint32_t* __restrict__ indices, const uint32_t* __restrict__ flags,
-                            const uint32_t* __restrict__ wpos, uint64_t m, uint2* __restrict__ words) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
-    const uint32_t x = indices[e];
-    const uint32_t p = wpos[e] - 1u;
-    if (flags[e]) words[p].x = x >> 5;
-    atomicOr(&words[p].y, 1u << (x & 31));
+                            const uint32_t* __restrict__ wpos, uint64_t m, uint2* __restrict__ words,
+                            const uint32_t* __restrict__ bad) {
+  if (*bad) return;
+  const uint64_t W = wpos[m - 1];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: warps keep their chunks aligned
+  for (uint64_t e = t0; e - lane < m; e += stride) {
+    const bool valid = e < m;
+    const uint32_t x = valid ? indices[e] : 0u;
+    const uint32_t p = valid ? wpos[e] - 1u : 0xffffffffu;
+    uint32_t v = valid ? 1u << (x & 31) : 0u;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_down_sync(FULLMASK, v, d);
+      const uint32_t po = __shfl_down_sync(FULLMASK, p, d);
+      if (lane + d < 32 && po == p) v |= o;
+    }
+    const uint32_t p_prev = __shfl_up_sync(FULLMASK, p, 1);
+    const uint32_t p_last = __shfl_sync(FULLMASK, p, 31);
+    if (!valid) continue;
+    if (e >= W) words[e] = make_uint2(0, 0);
+    if ((lane > 0 && p_prev == p) || !flags[e]) continue;  // not the opening edge of its pair
+    if (p_last == p) {  // the pair reaches the chunk's last edge: it may go on past the chunk
+      for (uint64_t k = e - lane + 32; k < m && !flags[k]; k++) v |= 1u << (indices[k] & 31);
+    }
+    words[p] = make_uint2(x >> 5, v);
   }
+  if (t0 < 2) words[m + t0] = make_uint2(0, 0);
 }
 
 // wptr[u] = first pair of row u (u in [0, n]); a row's first edge opens a pair.
 // desc[u]: the fused kernel's view of row u as a pivot, in one 16-byte load.
 __global__ void k_word_rowptr(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
                               const uint32_t* __restrict__ wpos, uint32_t n, uint64_t m, uint32_t* __restrict__ wptr,
-                              uint4* __restrict__ desc) {
+                              uint4* __restrict__ desc, const uint32_t* __restrict__ bad) {
+  if (*bad) return;
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= n; u += gridDim.x * blockDim.x) {
     const uint32_t e = indptr[u];
     const uint32_t w = (uint64_t)e < m ? wpos[e] - 1u : (m ? wpos[m - 1] : 0u);
@@ -343,9 +383,21 @@ __global__ void k_word_rowptr(const uint32_t* __restrict__ indptr, const uint32_
   }
 }
 
-// rev_indptr[v] = first position of key v in the sorted keys (v in [0, n]).
+// The reversed graph from the (column, forward edge id) pairs sorted by
+// column, in two passes (the row pointers' searches run with the whole
+// GPU's parallelism, not behind the gather in one grid-stride loop):
+// rev_cols[q] = source row of forward edge eids[q] (q < m) ...
+__global__ void k_gather(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ eids, uint64_t m,
+                         uint32_t* __restrict__ rev_cols, const uint32_t* __restrict__ bad) {
+  if (*bad) return;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) rev_cols[e] = rows[eids[e]];
+}
+
+// ... and rev_indptr[v] = first position of key v in the sorted keys (v <= n).
 __global__ void k_rev_indptr(const uint32_t* __restrict__ keys, uint64_t m, uint32_t n,
-                             uint32_t* __restrict__ rev_indptr) {
+                             uint32_t* __restrict__ rev_indptr, const uint32_t* __restrict__ bad) {
+  if (*bad) return;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += stride) {
     uint64_t lo = 0, hi = m;
@@ -355,18 +407,6 @@ __global__ void k_rev_indptr(const uint32_t* __restrict__ keys, uint64_t m, uint
     }
     rev_indptr[v] = (uint32_t)lo;
   }
-}
-
-__global__ void k_iota(uint32_t* __restrict__ a, uint64_t m) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) a[e] = (uint32_t)e;
-}
-
-// rev_cols[q] = row (source) of the forward edge eids[q]
-__global__ void k_gather(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, uint64_t m,
-                         uint32_t* __restrict__ dst) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) dst[e] = src[idx[e]];
 }
 
 inline uint64_t align4(uint64_t x) { return (x + 3) & ~3ull; }
@@ -415,7 +455,7 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
                 const uint32_t* d_rows, uint32_t n, uint64_t m, const std::vector<uint32_t>& cuts,
                 const uint32_t* d_cuts, const uint32_t* eids, const uint32_t* wpos, const uint32_t* wptr,
                 const uint32_t* fptr, const uint32_t* fidx, const uint2* words, uint32_t* d_stats,
-                uint64_t* d_coloff, int grid) {
+                uint64_t* d_coloff, const uint32_t* d_bad, int grid) {
   const uint32_t P = (uint32_t)cuts.size() - 1;
   const uint32_t T = P * P;
   cudaStream_t s = ctx->stream;
@@ -445,11 +485,10 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
     }
   }
   bt.stream = s;
-  DevBuf offs, counts, base, runs;
+  DevBuf offs, counts, runs;
   BBTC_TRY(dalloc(runs, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(offs, (T + P + 1) * sizeof(uint64_t), s));
   BBTC_TRY(dalloc(counts, bt.rp_len * sizeof(uint32_t), s));
-  BBTC_TRY(dalloc(base, T * sizeof(uint32_t), s));
   uint64_t* d_rp_off = offs.as<uint64_t>();
   uint64_t* d_part_off = d_rp_off + T;
   {
@@ -459,12 +498,17 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
     std::memcpy(h + T, part_off.data(), (P + 1) * sizeof(uint64_t));
     BBTC_CUDA(cudaMemcpyAsync(d_rp_off, h, (T + P + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
   }
-  BBTC_TRY(zero_fill(counts.p, bt.rp_len * sizeof(uint32_t), s, grid));
-  BBTC_TRY(zero_fill(bt.d_col, bt.col_len * sizeof(uint32_t), s, grid));
-  BBTC_CUDA(cudaMemsetAsync(d_stats, 0, 4 * T * sizeof(uint32_t), s));
+  {
+    // run counts, column pool, tile statistics and the row-pointer pool's
+    // 16-byte tail (every other slot of the pool is written below)
+    ZeroRanges z{{counts.as<uint32_t>(), bt.d_col, d_stats, bt.d_rp + part_off[P]},
+                 {bt.rp_len, bt.col_len, 4ull * T, bt.rp_len - part_off[P]}};
+    k_zero_ranges<<<grid, 256, 0, s>>>(z);
+    BBTC_CUDA(cudaGetLastError());
+  }
   if (m > 0) {
     k_entry_count<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, counts.as<uint32_t>(),
-                                       runs.as<uint32_t>());
+                                       runs.as<uint32_t>(), d_bad);
     BBTC_CUDA(cudaGetLastError());
     size_t rb = 0;
     BBTC_CUDA(cub::DeviceScan::InclusiveScan(nullptr, rb, runs.as<uint32_t>(), runs.as<uint32_t>(), cub::Max(),
@@ -474,40 +518,44 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
     BBTC_CUDA(cub::DeviceScan::InclusiveScan(rtmp.p, rb, runs.as<uint32_t>(), runs.as<uint32_t>(), cub::Max(),
                                              (int64_t)m, s));
   }
+  // run counts -> their inclusive scan, in place: k_localize_stats turns it into tile-local row pointers
   size_t tmp_bytes = 0;
-  BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, counts.as<uint32_t>(), bt.d_rp, (int64_t)bt.rp_len, s));
+  BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, counts.as<uint32_t>(), counts.as<uint32_t>(),
+                                          (int64_t)part_off[P], s));
   DevBuf tmp;
   BBTC_TRY(dalloc(tmp, tmp_bytes, s));
-  BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, counts.as<uint32_t>(), bt.d_rp, (int64_t)bt.rp_len, s));
-  k_tile_base<<<(T + 255) / 256, 256, 0, s>>>(bt.d_rp, d_rp_off, T, base.as<uint32_t>());
-  BBTC_CUDA(cudaGetLastError());
+  BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, counts.as<uint32_t>(), counts.as<uint32_t>(),
+                                          (int64_t)part_off[P], s));
   uint32_t* st_nnz = d_stats;
   uint32_t* st_max = d_stats + T;
   uint32_t* st_ne = d_stats + 2 * T;
-  k_localize_stats<<<grid, 256, 0, s>>>(bt.d_rp, counts.as<uint32_t>(), d_cuts, P, d_part_off, base.as<uint32_t>(),
-                                        part_off[P], st_max, st_ne);
+  k_localize_stats<<<grid, 256, 0, s>>>(bt.d_rp, counts.as<uint32_t>(), d_cuts, P, d_part_off, part_off[P], st_max,
+                                        st_ne, d_bad);
   BBTC_CUDA(cudaGetLastError());
-  k_tile_offsets<<<1, 32, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, st_nnz, d_coloff);
+  k_tile_offsets<<<1, 32, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, st_nnz, d_coloff, d_bad);
   BBTC_CUDA(cudaGetLastError());
   {
     uint32_t maxH = 1;
     for (uint32_t x = 0; x < P; x++) maxH = std::max(maxH, cuts[x + 1] - cuts[x]);
     const uint32_t gx = std::min<uint32_t>(64, (maxH + 255) / 256);
-    k_row_index<<<dim3(gx, T), 256, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, d_coloff, bt.d_erow);
+    k_row_index<<<dim3(gx, T), 256, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, d_coloff, bt.d_erow, d_bad);
     BBTC_CUDA(cudaGetLastError());
   }
   if (m > 0) {
     k_entry_scatter<<<grid, 256, 0, s>>>(runs.as<uint32_t>(), d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
                                          bt.d_col, eids, wpos, wptr, reinterpret_cast<uint2*>(bt.d_rec), fptr, fidx,
-                                         words);
+                                         words, d_bad);
     BBTC_CUDA(cudaGetLastError());
   }
   return BBTC_OK;
 }
 
-// Read back the tile statistics of one or two block CSRs (a may be null) with one sync.
+// Read back the tile statistics of one or two block CSRs (a may be null) with
+// one sync; with `d_bad`, also the input-contract flags (into *h_bad), and
+// when any is set the statistics are left unread.
 int fetch_stats(bbtc_ctx* ctx, BlockTiles* a, BlockTiles& b, const uint32_t* d_stats_a, const uint64_t* d_coloff_a,
-                const uint32_t* d_stats_b, const uint64_t* d_coloff_b, cudaStream_t s) {
+                const uint32_t* d_stats_b, const uint64_t* d_coloff_b, cudaStream_t s,
+                const uint32_t* d_bad = nullptr, uint32_t* h_bad = nullptr) {
   const uint32_t T = b.P * b.P;
   // pinned staging: [coloff a | coloff b | stats a | stats b]
   uint64_t* hc = reinterpret_cast<uint64_t*>(ctx->h_stage + kStageStats);
@@ -518,7 +566,13 @@ int fetch_stats(bbtc_ctx* ctx, BlockTiles* a, BlockTiles& b, const uint32_t* d_s
   }
   BBTC_CUDA(cudaMemcpyAsync(hc + T, d_coloff_b, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   BBTC_CUDA(cudaMemcpyAsync(hs + 3 * T, d_stats_b, 3 * T * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  uint32_t* hb = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageBad);
+  if (d_bad) BBTC_CUDA(cudaMemcpyAsync(hb, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   BBTC_CUDA(cudaStreamSynchronize(s));
+  if (d_bad) {
+    *h_bad = *hb;
+    if (*hb) return BBTC_OK;  // the statistics are void
+  }
   for (BlockTiles* p : {a, &b}) {
     if (!p) continue;
     const uint64_t* c = p == a ? hc : hc + T;
@@ -574,10 +628,50 @@ DevTile dev_tile(const BlockTiles& t, const std::vector<uint32_t>& cuts, uint32_
   return d;
 }
 
+// Layout scratch a context keeps between builds: the temporaries of a graph
+// of up to about five million edges (about 45 bytes per edge); a larger
+// build allocates its own and frees them at its end.
+constexpr size_t kScratchKeep = 256ull << 20;
+
+// Makes the context's kept scratch the running build's for the scope's
+// lifetime, then grows the kept block to what the build asked for (a quarter
+// more, at most kScratchKeep).  The kept block is a cache: when growing it
+// fails the next build allocates as before, so it bypasses the allocation
+// fault hook.  Its old block is freed behind the build's work on the stream.
+struct ScratchScope {
+  bbtc_ctx* ctx;
+  cudaStream_t s;
+  Scratch arena;
+  Scratch* prev;
+  ScratchScope(bbtc_ctx* c, cudaStream_t st) : ctx(c), s(st), prev(t_scratch) {
+    arena.base = c->d_scratch;
+    arena.cap = c->scratch_cap;
+    t_scratch = &arena;
+  }
+  ~ScratchScope() {
+    t_scratch = prev;
+    if (arena.want <= ctx->scratch_cap || arena.want > kScratchKeep) return;
+    if (ctx->d_scratch) cudaFreeAsync(ctx->d_scratch, s);
+    ctx->d_scratch = nullptr;
+    ctx->scratch_cap = 0;
+    const size_t cap = std::min(kScratchKeep, ((arena.want + arena.want / 4) + (1u << 20) - 1) & ~size_t((1u << 20) - 1));
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, cap, s) == cudaSuccess) {
+      ctx->d_scratch = static_cast<char*>(p);
+      ctx->scratch_cap = cap;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  ScratchScope(const ScratchScope&) = delete;
+  ScratchScope& operator=(const ScratchScope&) = delete;
+};
+
 int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_indices, bool host) {
   Range range("bbtc upload + layout");
   bbtc_ctx* ctx = g->ctx;
   cudaStream_t s = ctx->stream;
+  ScratchScope scratch(ctx, s);
   const uint32_t n = g->n;
   const uint64_t m = g->m;
   const uint32_t P = g->P;
@@ -621,13 +715,18 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     } ring{evs};
     uint32_t issued = 0;
     uint32_t by_kernel = 0;
+    auto mapped = [&](const void* src, size_t bytes) {
+      return host && bytes <= ctx->zero_copy_bytes && mapped_host_range(src, bytes);
+    };
+    // arrays that the SMs read over the host link, copied by one kernel launch
+    uint32_t* kdst[2] = {nullptr, nullptr};
+    const uint32_t* ksrc[2] = {nullptr, nullptr};
+    uint64_t kwords[2] = {0, 0};
     auto copy = [&](void* dst, const void* src, size_t bytes) -> int {
-      if (host && bytes <= ctx->zero_copy_bytes && mapped_host_range(src, bytes)) {
-        const uint64_t words = bytes / 4;
-        const uint64_t blocks = std::max<uint64_t>(1, (words + 4095) / 4096);
-        k_copy_mapped<<<(int)std::min<uint64_t>(blocks, 2ull * ctx->sms), 256, 0, s>>>(
-            static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(src), words);
-        BBTC_CUDA(cudaGetLastError());
+      if (mapped(src, bytes)) {
+        kdst[by_kernel] = static_cast<uint32_t*>(dst);
+        ksrc[by_kernel] = static_cast<const uint32_t*>(src);
+        kwords[by_kernel] = bytes / 4;
         by_kernel++;
         return BBTC_OK;
       }
@@ -647,46 +746,43 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     };
     BBTC_TRY(copy(g->d_indptr, in_indptr, ((size_t)n + 1) * sizeof(uint32_t)));
     if (m) BBTC_TRY(copy(g->d_indices, in_indices, m * sizeof(uint32_t)));
+    if (by_kernel) {
+      const uint64_t words = std::max(kwords[0], kwords[1]);
+      const uint64_t blocks = std::max<uint64_t>(1, (words + 4095) / 4096);
+      k_copy_mapped<<<(int)std::min<uint64_t>(blocks, 2ull * ctx->sms), 256, 0, s>>>(kdst[0], ksrc[0], kwords[0],
+                                                                                    kdst[1], ksrc[1], kwords[1]);
+      BBTC_CUDA(cudaGetLastError());
+    }
     g->zero_copy = by_kernel > 0;
   }
   const uint32_t* d_indptr = g->d_indptr;
   const uint32_t* d_indices = g->d_indices;
 
-  DevBuf d_cuts, bad, rows, stats_r, coloff_r, wflags, wpos;
+  DevBuf d_cuts, rows, stats_r, coloff_r, wflags, wpos, eids_in;
   BBTC_TRY(dalloc(wflags, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(wpos, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
-  BBTC_TRY(dalloc(d_cuts, g->cuts.size() * sizeof(uint32_t), s));
-  BBTC_TRY(dalloc(bad, sizeof(uint32_t), s));
+  BBTC_TRY(dalloc(d_cuts, (g->cuts.size() + 1) * sizeof(uint32_t), s));  // the cuts, then the contract flags
   BBTC_TRY(dalloc(rows, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(stats_r, 4 * T * sizeof(uint32_t), s));
   BBTC_TRY(dalloc(coloff_r, T * sizeof(uint64_t), s));
+  BBTC_TRY(dalloc(eids_in, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
+  uint32_t* d_bad = d_cuts.as<uint32_t>() + g->cuts.size();
   {
+    // one copy: the cut vector and a zero flags word
     uint32_t* h = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageCuts);
     std::memcpy(h, g->cuts.data(), g->cuts.size() * sizeof(uint32_t));
-    BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, h, g->cuts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    h[g->cuts.size()] = 0;
+    BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, h, (g->cuts.size() + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   }
-  BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
-  uint32_t hbad = 0;
+  // The contract check runs first; its flags are read back with the tile
+  // statistics at the end, and every kernel between that indexes by the input
+  // returns at once when they are set, so no host round trip splits the build.
   if (n > 0) {
-    // both checks, one read-back: nothing indexes by the input before it passes
-    k_validate_rows<<<grid, 256, 0, s>>>(d_indptr, n, m, bad.as<uint32_t>());
+    k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, rows.as<uint32_t>(), d_bad,
+                                        wflags.as<uint32_t>(), eids_in.as<uint32_t>());
     BBTC_CUDA(cudaGetLastError());
-    k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>(),
-                                        wflags.as<uint32_t>());
-    BBTC_CUDA(cudaGetLastError());
-    uint32_t* hb = reinterpret_cast<uint32_t*>(ctx->h_stage + kStageBad);
-    BBTC_CUDA(cudaMemcpyAsync(hb, bad.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    BBTC_CUDA(cudaStreamSynchronize(s));
-    hbad = *hb;
-  }
-  if (hbad) {
-    std::string why;
-    if (hbad & 1) why += " indptr[0] != 0;";
-    if (hbad & 2) why += " indptr[n] != m;";
-    if (hbad & 4) why += " row pointers decrease or exceed m;";
-    if (hbad & 8) why += " a column id >= n;";
-    if (hbad & 16) why += " a row is not strictly increasing (unsorted or duplicate ids);";
-    return fail(BBTC_ERR_INPUT, "CSR breaks the input contract:" + why);
+  } else if (m > 0) {
+    BBTC_CUDA(cudaMemsetAsync(d_bad, 0xff, sizeof(uint32_t), s));  // edges without rows
   }
 
   // the forward block CSR waits until something needs it (ensure_fwd): the
@@ -701,7 +797,6 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
       cudaGetLastError();
       return fail(BBTC_ERR_NOMEM, "device allocation of the word-compressed rows failed");
     }
-    BBTC_TRY(zero_fill(g->d_words, std::max<uint64_t>(m, 1) * sizeof(uint2) + 16, s, grid));
     if (m > 0) {
       size_t tb = 0;
       BBTC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, wflags.as<uint32_t>(), wpos.as<uint32_t>(), (int64_t)m, s));
@@ -709,26 +804,25 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
       BBTC_TRY(dalloc(tmp, tb, s));
       BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, wflags.as<uint32_t>(), wpos.as<uint32_t>(), (int64_t)m, s));
       k_word_fill<<<grid, 256, 0, s>>>(d_indices, wflags.as<uint32_t>(), wpos.as<uint32_t>(), m,
-                                       reinterpret_cast<uint2*>(g->d_words));
+                                       reinterpret_cast<uint2*>(g->d_words), d_bad);
       BBTC_CUDA(cudaGetLastError());
+    } else {
+      BBTC_CUDA(cudaMemsetAsync(g->d_words, 0, sizeof(uint2) + 16, s));
     }
     k_word_rowptr<<<grid, 256, 0, s>>>(d_indptr, d_indices, wpos.as<uint32_t>(), n, m, g->d_wptr,
-                                       static_cast<uint4*>(g->d_desc));
+                                       static_cast<uint4*>(g->d_desc), d_bad);
     BBTC_CUDA(cudaGetLastError());
   }
 
   // reversed graph: a stable sort of (column, forward edge id) by column keeps
   // every in-list ordered by source
   {
-    DevBuf eids_in, keys_out, eids_out, rev_indptr, rev_cols;
+    DevBuf keys_out, eids_out, rev_indptr, rev_cols;
     BBTC_TRY(dalloc(keys_out, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
-    BBTC_TRY(dalloc(eids_in, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
     BBTC_TRY(dalloc(eids_out, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
     BBTC_TRY(dalloc(rev_cols, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s));
     BBTC_TRY(dalloc(rev_indptr, ((size_t)n + 1) * sizeof(uint32_t), s));
     if (m > 0) {
-      k_iota<<<grid, 256, 0, s>>>(eids_in.as<uint32_t>(), m);
-      BBTC_CUDA(cudaGetLastError());
       int end_bit = 1;
       while (end_bit < 32 && (1ull << end_bit) < (uint64_t)n) end_bit++;
       size_t tmp_bytes = 0;
@@ -740,19 +834,35 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
       BBTC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, d_indices, keys_out.as<uint32_t>(),
                                                 eids_in.as<uint32_t>(), eids_out.as<uint32_t>(), (int64_t)m, 0,
                                                 end_bit, s));
-      k_gather<<<grid, 256, 0, s>>>(rows.as<uint32_t>(), eids_out.as<uint32_t>(), m, rev_cols.as<uint32_t>());
+    }
+    if (m > 0) {
+      k_gather<<<grid, 256, 0, s>>>(rows.as<uint32_t>(), eids_out.as<uint32_t>(), m, rev_cols.as<uint32_t>(), d_bad);
       BBTC_CUDA(cudaGetLastError());
     }
-    k_rev_indptr<<<grid, 256, 0, s>>>(keys_out.as<uint32_t>(), m, n, rev_indptr.as<uint32_t>());
+    k_rev_indptr<<<grid, 256, 0, s>>>(keys_out.as<uint32_t>(), m, n, rev_indptr.as<uint32_t>(), d_bad);
     BBTC_CUDA(cudaGetLastError());
     // reversed entries: row = column vertex v (keys), column = source u, record of forward edge (u, v)
     BBTC_TRY(build_block(ctx, g->rev, rev_indptr.as<uint32_t>(), rev_cols.as<uint32_t>(), keys_out.as<uint32_t>(),
                          n, m, g->cuts, d_cuts.as<uint32_t>(), eids_out.as<uint32_t>(), wpos.as<uint32_t>(),
                          g->d_wptr, d_indptr, d_indices, reinterpret_cast<const uint2*>(g->d_words),
-                         stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), grid));
+                         stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), d_bad, grid));
   }
-  // the host needs the tile statistics only now: one read-back for both block CSRs
-  BBTC_TRY(fetch_stats(ctx, nullptr, g->rev, nullptr, nullptr, stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), s));
+  // the host needs the tile statistics and the contract flags only now: one read-back
+  uint32_t hbad = 0;
+  BBTC_TRY(fetch_stats(ctx, nullptr, g->rev, nullptr, nullptr, stats_r.as<uint32_t>(), coloff_r.as<uint64_t>(), s,
+                       d_bad, &hbad));
+  if (hbad) {
+    std::string why;
+    if (hbad == 0xffffffffu) why += " edges but no rows;";
+    else {
+      if (hbad & 1) why += " indptr[0] != 0;";
+      if (hbad & 2) why += " indptr[n] != m;";
+      if (hbad & 4) why += " row pointers decrease or exceed m;";
+      if (hbad & 8) why += " a column id >= n;";
+      if (hbad & 16) why += " a row is not strictly increasing (unsorted or duplicate ids);";
+    }
+    return fail(BBTC_ERR_INPUT, "CSR breaks the input contract:" + why);
+  }
   BBTC_CUDA(cudaEventRecord(ev1, s));
   BBTC_CUDA(cudaEventSynchronize(ev1));
   float ms = 0;
@@ -784,16 +894,16 @@ int build_fwd(bbtc_graph* g) {
     std::memcpy(h, g->cuts.data(), g->cuts.size() * sizeof(uint32_t));
     BBTC_CUDA(cudaMemcpyAsync(d_cuts.p, h, g->cuts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   }
+  BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
   if (n > 0) {
     // row id of every edge (the CSR passed validation when it was uploaded)
-    BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
     k_expand_check<<<grid, 256, 0, s>>>(g->d_indptr, g->d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>(),
-                                        nullptr);
+                                        nullptr, nullptr);
     BBTC_CUDA(cudaGetLastError());
   }
   BBTC_TRY(build_block(ctx, g->fwd, g->d_indptr, g->d_indices, rows.as<uint32_t>(), n, m, g->cuts,
                        d_cuts.as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-                       stats.as<uint32_t>(), coloff.as<uint64_t>(), grid));
+                       stats.as<uint32_t>(), coloff.as<uint64_t>(), bad.as<uint32_t>(), grid));
   BBTC_TRY(fetch_stats(ctx, nullptr, g->fwd, nullptr, nullptr, stats.as<uint32_t>(), coloff.as<uint64_t>(), s));
   g->fwd_built = true;
   g->device_bytes += block_bytes(g->fwd, false);

@@ -144,6 +144,7 @@ Request* pick(bbtc_server* s, bool small_only) {
   AdmitLimits lim{s->opts.hbm_budget, s->in_use, s->opts.small_edges,
                   (uint64_t)s->opts.aging_ms * 1000000ull, now_ns(), small_only, kPickScan};
   lim.large_ok = !s->opts.max_large_loads || s->loading_large < s->opts.max_large_loads;
+  lim.small_aging_ns = (uint64_t)s->opts.small_aging_us * 1000ull;
   const size_t best = admit_pick(s->pending, lim);
   if (best == SIZE_MAX) return nullptr;
   Request* r = s->pending[best];

@@ -100,6 +100,9 @@ def parse():
                    help="serve: SMs of the small requests' partition (0: none; -1: the server's default)")
     p.add_argument("--max-large-loads", type=int, default=-1,
                    help="serve: large requests loading at once (0: no limit; -1: the server's default)")
+    p.add_argument("--small-aging-us", type=int, default=-1,
+                   help="serve: a small request waiting this long is loaded before smaller ones "
+                        "(0: the large requests' aging; -1: the server's default)")
     p.add_argument("--no-check", action="store_true", help="batch / serve: skip the oracle counts")
     p.add_argument("--no-batch", action="store_true", help="default line: no batched-launch sub-record")
     p.add_argument("--no-serve", action="store_true", help="default line: no serving sub-record")
@@ -504,7 +507,7 @@ def serve_once(srv, pool, max_scale: int, rate: float, duration: float, seed: in
 
 def measure_serve(max_scale: int, rates, duration: float, loaders: int, pin: bool, copy_engine_uploads: bool,
                   check: bool = True, trace=None, large_bps: int = 0, large_layout_bps: int = 0,
-                  max_large_loads: int = -1, small_sms: int = -1) -> dict:
+                  max_large_loads: int = -1, small_sms: int = -1, small_aging_us: int = -1) -> dict:
     """Pool generation, oracle counts of every pool graph, one warm-up
     request per scale, then one Poisson stream per rate on the same server."""
     from bbtc_b200 import Server
@@ -521,7 +524,8 @@ def measure_serve(max_scale: int, rates, duration: float, loaders: int, pin: boo
     srv = Server(0, loaders=loaders, copy_engine_uploads=copy_engine_uploads, large_blocks_per_sm=large_bps,
                  large_layout_blocks_per_sm=large_layout_bps,
                  max_large_loads=None if max_large_loads < 0 else max_large_loads,
-                 small_sms=None if small_sms < 0 else small_sms)
+                 small_sms=None if small_sms < 0 else small_sms,
+                 small_aging_us=None if small_aging_us < 0 else small_aging_us)
     try:
         for s in sorted(pool):
             g, c = pool[s][0]
@@ -537,6 +541,7 @@ def measure_serve(max_scale: int, rates, duration: float, loaders: int, pin: boo
             "oracle_s": round(oracle_s, 1), "launches": st.launches, "max_batch": st.max_batch,
             "loaders": loaders, "pinned_requests": pin, "large_blocks_per_sm": large_bps or 3,
             "large_layout_blocks_per_sm": large_layout_bps or 2, "small_sms": small_sms,
+            "small_aging_us": small_aging_us,
             "small_uploads": "copy engines" if copy_engine_uploads or not pin else "kernel reads",
             "workload": f"serving: Poisson arrivals, R-MAT scale 12+Geom(0.3) <= {max_scale}, ef 16"}
 
@@ -547,7 +552,7 @@ def run_serve(args):
     sv = measure_serve(args.serve_max_scale, rates, args.duration, args.loaders, bool(args.pin),
                        args.copy_engine_uploads, check=not args.no_check, trace=trace, large_bps=args.large_bps,
                        large_layout_bps=args.large_layout_bps, max_large_loads=args.max_large_loads,
-                       small_sms=args.small_sms)
+                       small_sms=args.small_sms, small_aging_us=args.small_aging_us)
     if args.trace:
         with open(args.trace, "w") as f:
             json.dump({"fields": ["scale", "m", "submit_ns", "load_ns", "ready_ns", "launch_ns", "done_ns", "batch"],
@@ -621,12 +626,13 @@ def main():
         # region and uncached, so every run tunes for the GPU it runs on
         from bbtc_b200 import autotune
         t0 = time.perf_counter()
-        o, tune_ms = autotune.sweep(st, base=o, bitmap_words=(768, 1024, 1536), occupancy=(5, 6),
-                                    warps_per_block=(8,), unit_work=(0,), repeats=5)
+        o, tune_ms = autotune.sweep(st, base=o, bitmap_words=(768, 1024, 1536), occupancy=(4, 5, 6),
+                                    warps_per_block=(8,), unit_work=(0, 512), repeats=5)
         o.use_cuda_graph = 1
         tuned = {f: getattr(o, f) for f in ("bitmap_words", "warps_per_block", "unit_work", "occupancy")}
         tuned.update(sweep_ms=round(tune_ms, 3), sweep_s=round(time.perf_counter() - t0, 2),
-                     space="bitmap_words 768/1024/1536 x occupancy 5/6, 8 warps, automatic units")
+                     space="bitmap_words 768/1024/1536 x occupancy 4/5/6 x units automatic / 512 probes, "
+                           "8 warps")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
     def timed_counts(opts, steps, warmup):

@@ -297,7 +297,8 @@ typedef struct bbtc_server_opts {
   uint32_t small_sms;       /* > 0: a partition of this many SMs (a multiple of 8; green contexts) runs the small
                                requests' loads and counts, the other SMs the large ones', so neither waits for
                                the other's blocks (0 = all SMs shared) */
-  uint32_t reserved;
+  uint32_t small_aging_us;  /* a small request waiting this long (microseconds) is loaded before smaller ones
+                               (0 = aging_ms) */
 } bbtc_server_opts;
 typedef struct bbtc_request_info {
   uint64_t count;     /* exact count once status == 1 */
