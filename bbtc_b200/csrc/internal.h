@@ -154,6 +154,7 @@ struct bbtc_ctx {
   size_t smem_optin = 0;
   uint32_t* d_unit_counter = nullptr;  // persistent-queue head (one word per launch slot)
   size_t smem_set = 0;                 // dynamic shared memory the count kernels are opted in to
+  bool open_carveout = false;          // layout kernels ask for the largest shared-memory carveout (launch_layout)
   uint32_t layout_blocks_per_sm = 8;   // grid cap of the layout kernels (256 threads a block)
   uint32_t upload_window = 0;          // host uploads: pieces in flight at most (0 = all at once)
   uint64_t zero_copy_bytes = 0;        // host arrays up to this size in mapped page-locked memory are read

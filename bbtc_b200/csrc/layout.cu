@@ -213,7 +213,11 @@ __global__ void k_localize_stats(uint32_t* __restrict__ rp, const uint32_t* __re
         tile = lo * P + y;
       }
     }
-    const uint32_t grp = __match_any_sync(FULLMASK, tile);
+    // a warp's 32 slots lie in one tile but at a tile's end: group lanes by
+    // tile only there (match and a per-group reduction are slow)
+    const uint32_t grp = __all_sync(FULLMASK, tile == __shfl_sync(FULLMASK, tile, 0))
+                             ? FULLMASK
+                             : __match_any_sync(FULLMASK, tile);
     const uint32_t mx = __reduce_max_sync(grp, rowlen);
     const uint32_t ne = __popc(grp & __ballot_sync(FULLMASK, rowlen != 0));
     if (tile != 0xffffffffu && lane == (uint32_t)(__ffs(grp) - 1)) {
@@ -223,18 +227,35 @@ __global__ void k_localize_stats(uint32_t* __restrict__ rp, const uint32_t* __re
   }
 }
 
-// nnz per tile and 16-byte aligned column offsets of the non-empty tiles (one block).
+// nnz per tile and 16-byte aligned column offsets of the non-empty tiles:
+// one warp, 32 tiles at a time, an exclusive scan of the aligned sizes by
+// shuffles (launched as one block of 32 threads).
 __global__ void k_tile_offsets(const uint32_t* __restrict__ rp, const uint64_t* __restrict__ rp_off,
                                const uint32_t* __restrict__ cuts, uint32_t P, uint32_t* __restrict__ nnz,
                                uint64_t* __restrict__ col_off, const uint32_t* __restrict__ bad) {
-  if (threadIdx.x != 0 || blockIdx.x != 0 || *bad) return;
+  if (blockIdx.x != 0 || threadIdx.x >= 32 || *bad) return;
+  const uint32_t lane = threadIdx.x;
+  const uint32_t T = P * P;
   uint64_t cur = 0;
-  for (uint32_t t = 0; t < P * P; t++) {
-    const uint32_t x = t / P;
-    const uint32_t z = rp[rp_off[t] + (cuts[x + 1] - cuts[x])];
-    nnz[t] = z;
-    col_off[t] = z ? cur : kNoSegment;
-    cur += ((uint64_t)z + 3) & ~3ull;
+  for (uint32_t t0 = 0; t0 < T; t0 += 32) {
+    const uint32_t t = t0 + lane;
+    uint32_t z = 0;
+    if (t < T) {
+      const uint32_t x = t / P;
+      z = rp[rp_off[t] + (cuts[x + 1] - cuts[x])];
+    }
+    const uint64_t size = ((uint64_t)z + 3) & ~3ull;
+    uint64_t incl = size;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint64_t o = __shfl_up_sync(FULLMASK, incl, d);
+      if (lane >= d) incl += o;
+    }
+    if (t < T) {
+      nnz[t] = z;
+      col_off[t] = z ? cur + incl - size : kNoSegment;
+    }
+    cur += __shfl_sync(FULLMASK, incl, 31);
   }
 }
 
@@ -447,6 +468,35 @@ bool mapped_host_range(const void* p, size_t bytes) {
   return size > 0 && b >= start && b + bytes <= (uint64_t)start + size;
 }
 
+// Launch of a layout kernel.  A context with `open_carveout` (the server's
+// large-request loaders) asks for the largest shared-memory carveout: an
+// SM's split between L1 and shared memory changes only when the SM is idle,
+// and a layout kernel (little shared memory of its own) otherwise runs with
+// a small carveout, so while one of its blocks holds an SM -- a large
+// graph's grid-stride pass runs a millisecond or more -- no block that needs
+// more shared memory (a CUB scan or sort pass of a small request's layout, a
+// count kernel) can start there, even from a higher-priority stream.  Other
+// contexts keep the driver's choice, which leaves the passes their L1
+// (R-MAT s22's layout is 2.8 ms slower with the largest carveout).
+template <typename... KArgs, typename... Args>
+int launch_layout(const bbtc_ctx* ctx, void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                  Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  if (ctx->open_carveout) {
+    attr[0].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+    attr[0].val.sharedMemCarveout = cudaSharedmemCarveoutMaxShared;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  BBTC_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+  return BBTC_OK;
+}
+
 // Build one block CSR (forward or reversed) from a CSR in device memory whose
 // per-edge row ids are `rows`.  With `eids` the reversed build also writes the
 // forward-edge records.  The tile statistics land in `st` (device, 4*P*P words)
@@ -503,13 +553,11 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
     // 16-byte tail (every other slot of the pool is written below)
     ZeroRanges z{{counts.as<uint32_t>(), bt.d_col, d_stats, bt.d_rp + part_off[P]},
                  {bt.rp_len, bt.col_len, 4ull * T, bt.rp_len - part_off[P]}};
-    k_zero_ranges<<<grid, 256, 0, s>>>(z);
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_zero_ranges, grid, 256, s, z));
   }
   if (m > 0) {
-    k_entry_count<<<grid, 256, 0, s>>>(d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off, counts.as<uint32_t>(),
-                                       runs.as<uint32_t>(), d_bad);
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_entry_count, grid, 256, s, d_indptr, d_indices, d_rows, m, d_cuts, P, d_rp_off,
+                           counts.as<uint32_t>(), runs.as<uint32_t>(), d_bad));
     size_t rb = 0;
     BBTC_CUDA(cub::DeviceScan::InclusiveScan(nullptr, rb, runs.as<uint32_t>(), runs.as<uint32_t>(), cub::Max(),
                                              (int64_t)m, s));
@@ -529,23 +577,20 @@ int build_block(bbtc_ctx* ctx, BlockTiles& bt, const uint32_t* d_indptr, const u
   uint32_t* st_nnz = d_stats;
   uint32_t* st_max = d_stats + T;
   uint32_t* st_ne = d_stats + 2 * T;
-  k_localize_stats<<<grid, 256, 0, s>>>(bt.d_rp, counts.as<uint32_t>(), d_cuts, P, d_part_off, part_off[P], st_max,
-                                        st_ne, d_bad);
-  BBTC_CUDA(cudaGetLastError());
-  k_tile_offsets<<<1, 32, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, st_nnz, d_coloff, d_bad);
-  BBTC_CUDA(cudaGetLastError());
+  BBTC_TRY(launch_layout(ctx, k_localize_stats, grid, 256, s, bt.d_rp, counts.as<uint32_t>(), d_cuts, P, d_part_off,
+                         part_off[P], st_max, st_ne, d_bad));
+  BBTC_TRY(launch_layout(ctx, k_tile_offsets, 1, 32, s, bt.d_rp, d_rp_off, d_cuts, P, st_nnz, d_coloff, d_bad));
   {
     uint32_t maxH = 1;
     for (uint32_t x = 0; x < P; x++) maxH = std::max(maxH, cuts[x + 1] - cuts[x]);
     const uint32_t gx = std::min<uint32_t>(64, (maxH + 255) / 256);
-    k_row_index<<<dim3(gx, T), 256, 0, s>>>(bt.d_rp, d_rp_off, d_cuts, P, d_coloff, bt.d_erow, d_bad);
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_row_index, dim3(gx, T), 256, s, bt.d_rp, d_rp_off, d_cuts, P, d_coloff, bt.d_erow,
+                           d_bad));
   }
   if (m > 0) {
-    k_entry_scatter<<<grid, 256, 0, s>>>(runs.as<uint32_t>(), d_indices, d_rows, m, d_cuts, P, d_rp_off, d_coloff, bt.d_rp,
-                                         bt.d_col, eids, wpos, wptr, reinterpret_cast<uint2*>(bt.d_rec), fptr, fidx,
-                                         words, d_bad);
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_entry_scatter, grid, 256, s, runs.as<uint32_t>(), d_indices, d_rows, m, d_cuts, P,
+                           d_rp_off, d_coloff, bt.d_rp, bt.d_col, eids, wpos, wptr,
+                           reinterpret_cast<uint2*>(bt.d_rec), fptr, fidx, words, d_bad));
   }
   return BBTC_OK;
 }
@@ -749,9 +794,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
     if (by_kernel) {
       const uint64_t words = std::max(kwords[0], kwords[1]);
       const uint64_t blocks = std::max<uint64_t>(1, (words + 4095) / 4096);
-      k_copy_mapped<<<(int)std::min<uint64_t>(blocks, 2ull * ctx->sms), 256, 0, s>>>(kdst[0], ksrc[0], kwords[0],
-                                                                                    kdst[1], ksrc[1], kwords[1]);
-      BBTC_CUDA(cudaGetLastError());
+      BBTC_TRY(launch_layout(ctx, k_copy_mapped, (int)std::min<uint64_t>(blocks, 2ull * ctx->sms), 256, s, kdst[0],
+                             ksrc[0], kwords[0], kdst[1], ksrc[1], kwords[1]));
     }
     g->zero_copy = by_kernel > 0;
   }
@@ -778,9 +822,8 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
   // statistics at the end, and every kernel between that indexes by the input
   // returns at once when they are set, so no host round trip splits the build.
   if (n > 0) {
-    k_expand_check<<<grid, 256, 0, s>>>(d_indptr, d_indices, n, m, rows.as<uint32_t>(), d_bad,
-                                        wflags.as<uint32_t>(), eids_in.as<uint32_t>());
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_expand_check, grid, 256, s, d_indptr, d_indices, n, m, rows.as<uint32_t>(), d_bad,
+                           wflags.as<uint32_t>(), eids_in.as<uint32_t>()));
   } else if (m > 0) {
     BBTC_CUDA(cudaMemsetAsync(d_bad, 0xff, sizeof(uint32_t), s));  // edges without rows
   }
@@ -803,15 +846,13 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
       DevBuf tmp;
       BBTC_TRY(dalloc(tmp, tb, s));
       BBTC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, wflags.as<uint32_t>(), wpos.as<uint32_t>(), (int64_t)m, s));
-      k_word_fill<<<grid, 256, 0, s>>>(d_indices, wflags.as<uint32_t>(), wpos.as<uint32_t>(), m,
-                                       reinterpret_cast<uint2*>(g->d_words), d_bad);
-      BBTC_CUDA(cudaGetLastError());
+      BBTC_TRY(launch_layout(ctx, k_word_fill, grid, 256, s, d_indices, wflags.as<uint32_t>(), wpos.as<uint32_t>(), m,
+                             reinterpret_cast<uint2*>(g->d_words), d_bad));
     } else {
       BBTC_CUDA(cudaMemsetAsync(g->d_words, 0, sizeof(uint2) + 16, s));
     }
-    k_word_rowptr<<<grid, 256, 0, s>>>(d_indptr, d_indices, wpos.as<uint32_t>(), n, m, g->d_wptr,
-                                       static_cast<uint4*>(g->d_desc), d_bad);
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_word_rowptr, grid, 256, s, d_indptr, d_indices, wpos.as<uint32_t>(), n, m,
+                           g->d_wptr, static_cast<uint4*>(g->d_desc), d_bad));
   }
 
   // reversed graph: a stable sort of (column, forward edge id) by column keeps
@@ -836,11 +877,11 @@ int build_layout(bbtc_graph* g, const uint32_t* in_indptr, const uint32_t* in_in
                                                 end_bit, s));
     }
     if (m > 0) {
-      k_gather<<<grid, 256, 0, s>>>(rows.as<uint32_t>(), eids_out.as<uint32_t>(), m, rev_cols.as<uint32_t>(), d_bad);
-      BBTC_CUDA(cudaGetLastError());
+      BBTC_TRY(launch_layout(ctx, k_gather, grid, 256, s, rows.as<uint32_t>(), eids_out.as<uint32_t>(), m,
+                             rev_cols.as<uint32_t>(), d_bad));
     }
-    k_rev_indptr<<<grid, 256, 0, s>>>(keys_out.as<uint32_t>(), m, n, rev_indptr.as<uint32_t>(), d_bad);
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_rev_indptr, grid, 256, s, keys_out.as<uint32_t>(), m, n, rev_indptr.as<uint32_t>(),
+                           d_bad));
     // reversed entries: row = column vertex v (keys), column = source u, record of forward edge (u, v)
     BBTC_TRY(build_block(ctx, g->rev, rev_indptr.as<uint32_t>(), rev_cols.as<uint32_t>(), keys_out.as<uint32_t>(),
                          n, m, g->cuts, d_cuts.as<uint32_t>(), eids_out.as<uint32_t>(), wpos.as<uint32_t>(),
@@ -897,9 +938,8 @@ int build_fwd(bbtc_graph* g) {
   BBTC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s));
   if (n > 0) {
     // row id of every edge (the CSR passed validation when it was uploaded)
-    k_expand_check<<<grid, 256, 0, s>>>(g->d_indptr, g->d_indices, n, m, rows.as<uint32_t>(), bad.as<uint32_t>(),
-                                        nullptr, nullptr);
-    BBTC_CUDA(cudaGetLastError());
+    BBTC_TRY(launch_layout(ctx, k_expand_check, grid, 256, s, g->d_indptr, g->d_indices, n, m, rows.as<uint32_t>(),
+                           bad.as<uint32_t>(), nullptr, nullptr));
   }
   BBTC_TRY(build_block(ctx, g->fwd, g->d_indptr, g->d_indices, rows.as<uint32_t>(), n, m, g->cuts,
                        d_cuts.as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,

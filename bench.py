@@ -46,10 +46,10 @@ METRIC = "edges/sec at exact count, batched vs plain form on 1 B200; p50/p99 lat
 UNIT = "edges/s"
 FALLBACK_HBM_GBS = 6650.0
 # serving throughput peak on one B200: requests/s served when the offered
-# rate exceeds what the server sustains (1,800 req/s offered: 1,508-1,527
-# served, 4.58e9-4.68e9 edges/s, three runs); the default line serves at 80 %
-# of it
-SERVE_PEAK_RPS = 1510.0
+# rate exceeds what the server sustains, with the server's default
+# configuration (1,800 req/s offered for 30 s: 1,450 and 1,454 served,
+# 4.44e9-4.45e9 edges/s, two runs); the default line serves at 80 % of it
+SERVE_PEAK_RPS = 1450.0
 
 
 def parse():
@@ -87,7 +87,7 @@ def parse():
     p.add_argument("--rate", type=float, default=600.0, help="serve: requests per second")
     p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     p.add_argument("--serve-max-scale", type=int, default=22)
-    p.add_argument("--loaders", type=int, default=4, help="serve: loader threads")
+    p.add_argument("--loaders", type=int, default=6, help="serve: loader threads")
     p.add_argument("--pin", type=int, default=1, help="serve: request buffers in page-locked host memory")
     p.add_argument("--copy-engine-uploads", action="store_true",
                    help="serve: small requests go through the copy engines even from page-locked buffers")

@@ -281,7 +281,7 @@ typedef struct bbtc_server_opts {
   uint64_t hbm_budget;    /* device bytes admitted graphs may hold (0 = 150 GiB) */
   uint32_t max_batch;     /* graphs per launch (0 = 4096) */
   uint32_t max_requests;  /* requests held (queued, running or finished, not released) (0 = 2^20) */
-  uint32_t loaders;       /* loader threads, each with its own stream (0 = 2) */
+  uint32_t loaders;       /* loader threads, each with its own stream (0 = 6) */
   uint32_t copy_engine_uploads; /* 1: small requests' CSRs always go through the copy engines; 0 (default):
                                    from page-locked host buffers they are read by a kernel
                                    (bbtc_ctx_set_zero_copy) */
@@ -293,7 +293,7 @@ typedef struct bbtc_server_opts {
                              wait for it to grow (0 = 1.1 x hbm_budget; at most the free memory less 8 GiB) */
   uint32_t large_layout_blocks_per_sm; /* grid cap of the large requests' layout kernels, blocks of 256 threads per
                                           SM (0 = 2), so that small requests' kernels find room on every SM */
-  uint32_t max_large_loads; /* large requests uploaded and laid out at once, at most (0 = no limit) */
+  uint32_t max_large_loads; /* large requests uploaded and laid out at once, at most (default 2; 0 = no limit) */
   uint32_t small_sms;       /* > 0: a partition of this many SMs (a multiple of 8; green contexts) runs the small
                                requests' loads and counts, the other SMs the large ones', so neither waits for
                                the other's blocks (0 = all SMs shared) */
