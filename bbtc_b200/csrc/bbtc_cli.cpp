@@ -11,8 +11,6 @@
 //                no task goes to a CPU worker.
 //   --copy-first the block CSR is device-resident from the layout build on, so
 //                the "Copy tiles to device (s)" field measures a stream sync.
-//   --partitioner rac is accepted and served by the pal cuts (the count does
-//                not depend on the cuts).
 #include <omp.h>
 #include <sys/stat.h>
 
@@ -234,8 +232,8 @@ int main(int argc, const char** argv) {
   try {
     bbtc::Context ctx(0);
     const uint32_t P = (uint32_t)params.ncut;
-    // pal, the default (rac served by pal)
-    const int pk = params.part_name == "uni" ? 0 : params.part_name == "n1d" ? 1 : 2;
+    // pal, the default
+    const int pk = params.part_name == "uni" ? 0 : params.part_name == "n1d" ? 1 : params.part_name == "rac" ? 4 : 2;
     std::vector<uint32_t> cuts(P + 1);
     RegionBegin();
     bbtc::check(bbtcp_cuts(pk, n, indptr.data(), indices.data(), P, 1091467301ull, cuts.data()));

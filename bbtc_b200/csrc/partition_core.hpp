@@ -33,20 +33,24 @@ void uniform_cuts(uint32_t n, uint32_t P, uint32_t* cuts) {
   for (uint32_t i = 0; i <= P; i++) cuts[i] = (uint32_t)((uint64_t)i * n / P);
 }
 
-// greedy: can rows be split into <= P stripes of nnz <= B?
-bool n1d_probe(uint32_t n, const uint32_t* indptr, uint32_t P, uint64_t B, uint32_t* cuts) {
+// Greedy probe over a prefix-sum array (n + 1 nondecreasing entries): can
+// [0, n) be split into <= P contiguous parts whose sums are <= B?  Each cut is
+// the furthest position whose part stays within B; with `cuts`, they are
+// written, and unused parts are empty at the end.
+template <class T>
+bool prefix_probe(uint32_t n, const T* prefix, uint32_t P, uint64_t B, uint32_t* cuts) {
   uint32_t start = 0;
   uint32_t k = 0;
   if (cuts) cuts[0] = 0;
   while (start < n) {
     if (k == P) return false;
-    // furthest end with indptr[end] - indptr[start] <= B
-    const uint64_t limit = (uint64_t)indptr[start] + B;
-    const uint32_t* it = std::upper_bound(indptr + start, indptr + n + 1, limit,
-                                          [](uint64_t v, uint32_t e) { return v < e; });
-    uint32_t end = (uint32_t)(it - indptr) - 1;  // last index with indptr <= limit
-    if (end <= start) end = start + 1;           // a single row heavier than B
-    if ((uint64_t)indptr[end] - indptr[start] > B) return false;
+    // furthest end with prefix[end] - prefix[start] <= B
+    const uint64_t limit = (uint64_t)prefix[start] + B;
+    const T* it = std::upper_bound(prefix + start, prefix + n + 1, limit,
+                                   [](uint64_t v, T e) { return v < (uint64_t)e; });
+    uint32_t end = (uint32_t)(it - prefix) - 1;  // last index with prefix <= limit
+    if (end <= start) end = start + 1;           // a single element heavier than B
+    if ((uint64_t)prefix[end] - prefix[start] > B) return false;
     start = end;
     k++;
     if (cuts) cuts[k] = start;
@@ -56,20 +60,29 @@ bool n1d_probe(uint32_t n, const uint32_t* indptr, uint32_t P, uint64_t B, uint3
   return true;
 }
 
-void n1d_cuts(uint32_t n, const uint32_t* indptr, uint32_t P, uint32_t* cuts) {
-  uint64_t lo = 0, hi = indptr[n];
-  uint64_t maxrow = 0;
-  for (uint32_t i = 0; i < n; i++) maxrow = std::max<uint64_t>(maxrow, indptr[i + 1] - indptr[i]);
-  lo = std::max<uint64_t>(maxrow, (indptr[n] + P - 1) / P);
-  if (lo > hi) hi = lo;
+// The optimal P-way contiguous split of a prefix-sum array (Nicol, JPDC 1994:
+// the smallest largest part): a binary search on the bound with the greedy
+// probe, whose cuts at the optimal bound are returned.
+template <class T>
+void prefix_cuts(uint32_t n, const T* prefix, uint32_t P, uint32_t* cuts) {
+  uint64_t maxel = 0;
+  for (uint32_t i = 0; i < n; i++) maxel = std::max<uint64_t>(maxel, (uint64_t)prefix[i + 1] - prefix[i]);
+  const uint64_t total = (uint64_t)prefix[n] - prefix[0];
+  uint64_t lo = std::max<uint64_t>(maxel, (total + P - 1) / P), hi = std::max<uint64_t>(lo, total);
   while (lo < hi) {
     const uint64_t mid = lo + (hi - lo) / 2;
-    if (n1d_probe(n, indptr, P, mid, nullptr)) hi = mid; else lo = mid + 1;
+    if (prefix_probe(n, prefix, P, mid, nullptr)) hi = mid; else lo = mid + 1;
   }
-  n1d_probe(n, indptr, P, lo, cuts);
-  // spread any unused stripes as empty parts at the end
+  prefix_probe(n, prefix, P, lo, cuts);
   cuts[P] = n;
 }
+
+// greedy: can rows be split into <= P stripes of nnz <= B?
+bool n1d_probe(uint32_t n, const uint32_t* indptr, uint32_t P, uint64_t B, uint32_t* cuts) {
+  return prefix_probe(n, indptr, P, B, cuts);
+}
+
+void n1d_cuts(uint32_t n, const uint32_t* indptr, uint32_t P, uint32_t* cuts) { prefix_cuts(n, indptr, P, cuts); }
 
 struct Sample {
   std::vector<uint32_t> row_ptr;  // sampled nonzeros bucketed by row (CSR over n)
@@ -365,6 +378,81 @@ void pal_cuts_fast(uint32_t n, const uint32_t* indptr, const uint32_t* indices, 
     cols[t] = indices[es[t]];
   }
   pal_from_sample(n, P, rows, cols, cuts);
+}
+
+// ---- rac: refine a cut ------------------------------------------------------
+//
+// Symmetric cuts refined one direction at a time (SARMA
+// algorithms/refine_a_cut.hpp:43-70, :129-186): given the current cuts, a
+// row's weight is its largest count of nonzeros inside one column part; the
+// new cuts are the optimal contiguous split of those weights (prefix_cuts).
+// The direction is the rows of A or of its transpose, whichever gives the
+// smaller largest tile after one refinement from the trivial cuts
+// [0, n, ..., n]; that direction is then refined max(10, P) times.
+
+// Row weights under column cuts `cut` (P + 1 entries, nondecreasing, cut[0] =
+// 0, every id < cut[P]), summed into prefix (n + 1 entries).
+void rac_weights(uint32_t n, const uint32_t* ptr, const uint32_t* idx, const std::vector<uint32_t>& cut,
+                 std::vector<uint64_t>& prefix) {
+  prefix.assign((size_t)n + 1, 0);
+  for (uint32_t i = 0; i < n; i++) {
+    uint64_t best = 0, run = 0;
+    size_t k = 1;  // the current column part is [cut[k - 1], cut[k])
+    for (uint32_t e = ptr[i]; e < ptr[i + 1]; e++) {
+      while (idx[e] >= cut[k]) {
+        best = std::max(best, run);
+        run = 0;
+        k++;
+      }
+      run++;
+    }
+    prefix[i + 1] = prefix[i] + std::max(best, run);
+  }
+}
+
+// Largest tile nnz of A under the symmetric cuts.
+uint64_t rac_maxload(uint32_t n, const uint32_t* indptr, const uint32_t* indices, const std::vector<uint32_t>& cut) {
+  const size_t P = cut.size() - 1;
+  std::vector<uint64_t> tile(P * P, 0);
+  size_t x = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    while (i >= cut[x + 1]) x++;
+    for (uint32_t e = indptr[i]; e < indptr[i + 1]; e++) {
+      const size_t y = (size_t)(std::upper_bound(cut.begin(), cut.end(), indices[e]) - cut.begin()) - 1;
+      tile[x * P + y]++;
+    }
+  }
+  return tile.empty() ? 0 : *std::max_element(tile.begin(), tile.end());
+}
+
+void rac_cuts(uint32_t n, const uint32_t* indptr, const uint32_t* indices, uint32_t P, uint32_t* cuts) {
+  // the transpose, rows sorted (a counting sort by column, rows in order)
+  const uint64_t m = indptr[n];
+  std::vector<uint32_t> tptr((size_t)n + 1, 0), tidx(m);
+  for (uint64_t e = 0; e < m; e++) tptr[indices[e] + 1]++;
+  for (uint32_t i = 0; i < n; i++) tptr[i + 1] += tptr[i];
+  {
+    std::vector<uint32_t> fill(tptr.begin(), tptr.end() - 1);
+    for (uint32_t i = 0; i < n; i++)
+      for (uint32_t e = indptr[i]; e < indptr[i + 1]; e++) tidx[fill[indices[e]]++] = i;
+  }
+  std::vector<uint64_t> prefix;
+  auto refine = [&](bool transposed, const std::vector<uint32_t>& prev) {
+    if (transposed) rac_weights(n, tptr.data(), tidx.data(), prev, prefix);
+    else rac_weights(n, indptr, indices, prev, prefix);
+    std::vector<uint32_t> next(prev.size());
+    prefix_cuts(n, prefix.data(), (uint32_t)prev.size() - 1, next.data());
+    return next;
+  };
+  std::vector<uint32_t> start(P + 1, n);
+  start[0] = 0;
+  const uint64_t load_rows = rac_maxload(n, indptr, indices, refine(false, start));
+  const uint64_t load_cols = rac_maxload(n, indptr, indices, refine(true, start));
+  const bool transposed = load_cols < load_rows;
+  std::vector<uint32_t> cur = start;
+  const uint32_t iters = std::max<uint32_t>(10, P);
+  for (uint32_t it = 0; it < iters; it++) cur = refine(transposed, cur);
+  std::copy(cur.begin(), cur.end(), cuts);
 }
 
 }  // namespace

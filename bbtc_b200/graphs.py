@@ -156,13 +156,13 @@ def from_pairs(n: int, src, dst, name: str = "pairs") -> OrientedCSR:
     return _take(h, name, dict(kind="pairs"))
 
 
-PARTITIONERS = {"uni": 0, "n1d": 1, "pal": 2, "pal-bisect": 3}  # pal-bisect: same cuts as pal, slower probe
+PARTITIONERS = {"uni": 0, "n1d": 1, "pal": 2, "pal-bisect": 3, "rac": 4}  # pal-bisect: same cuts as pal, slower probe
 PAL_SEED = 1091467301  # the sampling seed the reference passes (include/utils/utils.hpp:272)
 
 
 def cuts(g: OrientedCSR, ncut: int, partitioner: str = "pal", seed: int = PAL_SEED) -> np.ndarray:
     """Symmetric cut vector (ncut+1 entries, cuts[0]=0, cuts[-1]=n) from the
-    uni / n1d / pal partitioners (bbtc_b200/csrc/partition.cpp)."""
+    uni / n1d / pal / rac partitioners (bbtc_b200/csrc/partition.cpp)."""
     if partitioner not in PARTITIONERS:
         raise ValueError(f"unknown partitioner {partitioner!r}; expected one of {sorted(PARTITIONERS)}")
     if ncut < 1:

@@ -2,7 +2,8 @@
 code gives for them.
 
 Run in a container that has the reference tree (oracle/_ref built from it):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # everything
+    python tests/golden/make_golden.py --rac    # sarma-rac-cuts.npz only
 Each fixture holds the oriented CSR (indptr, indices), and for every cut vector
 (`cuts_<part>_<P>`) the count of the reference's CPU path compiled from its
 sources (oracle.ref_count).  `cli_triangles` / `cli_edges` come from the
@@ -62,5 +63,48 @@ def main():
         print(f"{g.name}: n={g.n} m={g.m} triangles={int(out['count_uni_1'])}")
 
 
+# Graphs whose rac cuts are pinned (sarma-rac-cuts.npz): regenerated from
+# these calls by the test, so only the cut vectors are stored.
+RAC_CASES = {
+    "rmat-s12-ef16-seed3": lambda: graphs.rmat(12, 16, seed=3),
+    "rmat-s14-ef8-seed5": lambda: graphs.rmat(14, 8, seed=5),
+    "chunglu-n8192-seed6": lambda: graphs.chung_lu(1 << 13, seed=6, max_deg=400.0),
+}
+RAC_P = (3, 8, 16, 33)
+
+
+def _ref_rac_child(key, P):
+    g = RAC_CASES[key]()
+    print(" ".join(str(int(c)) for c in oracle.ref_cuts(g.n, g.indptr, g.indices, P, "rac")))
+
+
+def rac_main():
+    """SARMA's rac cuts (refine_a_cut::partition, the reference's call
+    sequence in oracle/_ref) for RAC_CASES x RAC_P.  Each runs in a child
+    process, retried: SARMA's parallel loops crashed the process now and then
+    (a segmentation fault inside the reference's code, not reproducible on
+    its own)."""
+    import subprocess
+    out = {}
+    for key in RAC_CASES:
+        for P in RAC_P:
+            for attempt in range(5):
+                r = subprocess.run([sys.executable, os.path.abspath(__file__), "--rac-child", key, str(P)],
+                                   capture_output=True, text=True)
+                if r.returncode == 0:
+                    break
+            else:
+                raise SystemExit(f"SARMA rac failed for {key} P={P}: {r.stderr[-300:]}")
+            out[f"{key}__{P}"] = np.array([int(x) for x in r.stdout.split()], dtype=np.uint32)
+            print(key, P, "attempts", attempt + 1)
+    np.savez_compressed(os.path.join(HERE, "sarma-rac-cuts.npz"), **out)
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "--rac-child":
+        _ref_rac_child(sys.argv[2], int(sys.argv[3]))
+    elif len(sys.argv) > 1 and sys.argv[1] == "--rac":
+        rac_main()
+    else:
+        main()
+        rac_main()

@@ -2,6 +2,8 @@
 reference's own CPU path (compiled from its sources into oracle/_ref), the
 reference's unmodified executable, and closed-form / brute-force counts."""
 import math
+import os
+import sys
 
 import numpy as np
 import pytest
@@ -186,3 +188,23 @@ def test_partitioners_against_sarma(make, P):
     ours = int(oracle.tile_nnz(g.n, g.indptr, g.indices, pal).max())
     theirs = int(oracle.tile_nnz(g.n, g.indptr, g.indices, ref_pal).max())
     assert ours <= 1.15 * theirs, (ours, theirs)
+
+
+
+def test_rac_equals_sarma():
+    """rac (refine a cut) is deterministic: the library's cuts equal SARMA's
+    (refine_a_cut::partition on the whole matrix, the reference's call
+    sequence of utils.hpp:282-283, run by tests/golden/make_golden.py --rac),
+    except the last cut (n here, n + 1 in the reference).  The reference's
+    cuts are fixtures: its rac crashed the test process now and then (a
+    segmentation fault inside SARMA's parallel loops)."""
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import RAC_CASES, RAC_P
+    ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sarma-rac-cuts.npz"))
+    for key, make in RAC_CASES.items():
+        g = make()
+        for P in RAC_P:
+            theirs = ref[f"{key}__{P}"]
+            ours = graphs.cuts(g, P, "rac")
+            assert np.array_equal(ours[:-1], theirs[:-1]), (key, P, ours, theirs)
+            assert ours[-1] == g.n and theirs[-1] == g.n + 1
