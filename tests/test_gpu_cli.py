@@ -47,6 +47,8 @@ def test_edge_list_and_cache(tmp_path):
     out2 = run("--graph", path, "--ncut", "5", "--partitioner", "n1d", "--copy-first", "--repeat", "1")
     assert field(out2, "Number of Triangles:") == want
     assert "Copy tiles to device (s) : " in out2
+    out3 = run("--graph", path, "--ncut", "6", "--partitioner", "rac", "--repeat", "1")
+    assert field(out3, "Number of Triangles:") == want
 
 
 def test_matrix_market_one_based(tmp_path):
