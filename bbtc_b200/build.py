@@ -23,7 +23,7 @@ BIN = os.path.join(HERE, "bin")
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("BBTC_CXX", shutil.which("g++") or "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["api.cu", "layout.cu", "count.cu", "server.cu", "prep.cu", "partition_dev.cu"]
+CUDA_SOURCES = ["api.cu", "layout.cu", "count.cu", "server.cu", "prep.cu", "partition_dev.cu", "hybrid.cpp"]
 HOST_SOURCES = ["graphgen.cpp", "partition.cpp", "graph_io.cpp"]
 
 

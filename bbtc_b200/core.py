@@ -55,6 +55,12 @@ class GraphInfo(c.Structure):
                 ("layout_ms", c.c_double), ("zero_copy", c.c_uint32), ("reserved", c.c_uint32)]
 
 
+class HybridStats(c.Structure):
+    _fields_ = [("gpu_tasks", c.c_uint32), ("cpu_tasks", c.c_uint32), ("gpu_launches", c.c_uint32),
+                ("separator", c.c_uint32), ("gpu_count", c.c_uint64), ("cpu_count", c.c_uint64),
+                ("gpu_ms", c.c_double), ("cpu_ms", c.c_double)]
+
+
 TASK_DTYPE = np.dtype([("ab", np.uint32), ("bc", np.uint32), ("ac", np.uint32)])
 
 _typed = False
@@ -89,6 +95,8 @@ def lib() -> ctypes.CDLL:
         "bbtc_count_wait": [vp, vp, c.POINTER(u64)],
         "bbtc_last_launches": [vp, c.POINTER(u32)],
         "bbtc_count_batch": [vp, vp, u32, c.POINTER(Opts), vp],
+        "bbtc_count_hybrid": [vp, vp, vp, vp, vp, u32, i32, u32, c.POINTER(Opts), c.POINTER(u64),
+                              c.POINTER(HybridStats)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -283,6 +291,21 @@ class Graph:
                                c.byref(out)))
         return out.value
 
+    def count_hybrid(self, indptr, indices, tasks: np.ndarray | None = None, border: int = 0, cpu_workers: int = 1,
+                     opts: Opts | None = None) -> tuple[int, dict]:
+        """The count with CPU workers beside the GPU (bb_tc.cpp:142-252):
+        tasks [0, Separator) on the GPU, the rest shared -- CPU workers from
+        the tail, the GPU from the head.  indptr / indices: the host CSR this
+        graph was uploaded from.  Returns (count, stats)."""
+        ip = _u32(indptr)
+        ix = _u32(indices) if len(indices) else np.zeros(1, np.uint32)
+        out = c.c_uint64()
+        st = HybridStats()
+        tp, nt = _tasks_arg(tasks)
+        check(lib().bbtc_count_hybrid(self.ctx.handle, self.handle, ip.ctypes.data, ix.ctypes.data, tp, nt, border,
+                                      cpu_workers, c.byref(opts) if opts else None, c.byref(out), c.byref(st)))
+        return out.value, {f: getattr(st, f) for f, _ in HybridStats._fields_}
+
     def count_async(self, tasks: np.ndarray | None = None, border: int = -1, opts: Opts | None = None) -> None:
         tp, nt = _tasks_arg(tasks)
         check(lib().bbtc_count_async(self.ctx.handle, self.handle, tp, nt, border, c.byref(opts) if opts else None))
@@ -335,7 +358,10 @@ def count_batch(ctx: Context, graphs: list[Graph], opts: Opts | None = None) -> 
 
 class BBTc:
     """The reference's driver object (include/triangle_counting/bb_tc.h:28-218)
-    over the device layout: same method names, GPU only."""
+    over the device layout: same method names.  By default every task runs on
+    the GPU; SetCpuWorkers(k, indptr, indices) adds k CPU workers that take
+    tasks past the Separator from the tail, as the reference's OpenMP workers
+    do (bb_tc.cpp:184-197)."""
 
     def __init__(self, st: Graph, tasks: np.ndarray | None = None, P: int | None = None):
         if P is not None and P != st.P:
@@ -345,6 +371,18 @@ class BBTc:
         self.Separator = -1
         self.opts = options()
         self._ngpu = 1
+        self._cpu = 0
+        self._host = None
+        self.last_stats: dict | None = None
+
+    def SetCpuWorkers(self, k: int, indptr=None, indices=None) -> None:
+        """k CPU workers beside the GPU; they read the host CSR the graph was uploaded from."""
+        if k < 0:
+            raise BBTcError(-1, "the number of CPU workers must be >= 0")
+        if k > 0 and (indptr is None or indices is None):
+            raise BBTcError(-1, "CPU workers need the host CSR (indptr, indices)")
+        self._cpu = k
+        self._host = (_u32(indptr), _u32(indices)) if k > 0 else None
 
     # InitFlags / ResetFlags / PrepareGpu / CopyTilesToGpu have nothing to do:
     # the queue lives on the device and the tiles are resident after upload.
@@ -369,6 +407,11 @@ class BBTc:
         return self._ngpu
 
     def NoOfTriangles(self) -> int:
+        if self._cpu > 0:
+            sep = -1 if self.Separator is None else int(self.Separator)
+            count, self.last_stats = self.st.count_hybrid(self._host[0], self._host[1], self.tasks,
+                                                          max(sep, -2), self._cpu, self.opts)
+            return count
         border = -1 if self.Separator is None or self.Separator < 0 or self.Separator >= len(self.tasks) \
             else int(self.Separator)
         return self.st.count(self.tasks, border, self.opts)

@@ -2,18 +2,22 @@
 //
 // Same flags, defaults, checks and output lines as the reference's CUDA driver
 // (argument parsing include/utils/utils.hpp:21-154, main src/bbtc.cu:15-90,
-// timing fields include/utils/hooks.hpp:13-56).  Differences, all forced by
-// "one GPU, no CPU workers":
+// timing fields include/utils/hooks.hpp:13-56).  Differences, forced by
+// "one GPU" or added:
 //   --ngpu       only 1 is served (the default "all devices" means 1); 0 (CPU
 //                only) and > 1 print a message and exit like other bad input.
 //   --nstream    accepted and checked; the persistent kernel uses one stream.
-//   --border     keeps its meaning for the queue order (tasks [0, b) first);
-//                no task goes to a CPU worker.
+//   --border     tasks [0, b) run on the GPU only; the rest are shared with
+//                CPU workers when there are any (bb_tc.cpp:142-252).
+//   --cpu-workers (added) CPU worker threads beside the GPU: 0 (default) =
+//                every task on the GPU; -1 = the reference's split, OpenMP
+//                threads minus the --nstream GPU workers.
 //   --copy-first the block CSR is device-resident from the layout build on, so
 //                the "Copy tiles to device (s)" field measures a stream sync.
 #include <omp.h>
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <chrono>
 #include <climits>
 #include <cstdint>
@@ -48,6 +52,7 @@ struct Parameters {
   int border = 0;
   int ncut = 32;
   int repeat = 5;
+  int cpu_workers = 0;
   bool copy_first = false;
 };
 
@@ -90,6 +95,8 @@ void PrintUsage() {
   std::cout << "                          Note: Cannot be 0." << std::endl;
   std::cout << "  --border <int>        Work queue border for GPUs                 (|T|/2)" << std::endl;
   std::cout << "                          Note: if set to -1, GPUs process all." << std::endl;
+  std::cout << "  --cpu-workers <int>   CPU workers beside the GPU                 (0)" << std::endl;
+  std::cout << "                          Note: -1 = threads minus GPU streams." << std::endl;
   std::cout << "  --copy-first          If set then copy graph to GPUs first       (false)" << std::endl;
   std::cout << "  --repeat <int>        Run bbTC algorithm '--repeat' times        (5)" << std::endl;
   std::cout << std::endl;
@@ -149,6 +156,9 @@ void ParseArguments(Parameters& p, int argc, const char** argv, int devices) {
     } else if (a == "--border") {
       p.border = ToInt(next());
       CheckIntParams("--border", p.border, -2);
+    } else if (a == "--cpu-workers") {
+      p.cpu_workers = ToInt(next());
+      CheckIntParams("--cpu-workers", p.cpu_workers, -1);
     } else if (a == "--repeat") {
       p.repeat = ToInt(next());
       CheckIntParams("--repeat", p.repeat);
@@ -262,6 +272,12 @@ int main(int argc, const char** argv) {
       bb.Separator = (int)t_list.size() / 2;
     else
       bb.Separator = params.border;
+
+    if (params.cpu_workers != 0) {
+      const int k = params.cpu_workers > 0 ? params.cpu_workers
+                                           : std::max(0, omp_get_max_threads() - params.n_stream * params.n_gpu);
+      bb.SetCpuWorkers((uint32_t)k, indptr, indices);
+    }
 
     RegionBegin();
     bb.PrepareGpu();

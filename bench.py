@@ -106,6 +106,7 @@ def parse():
     p.add_argument("--no-check", action="store_true", help="batch / serve: skip the oracle counts")
     p.add_argument("--no-batch", action="store_true", help="default line: no batched-launch sub-record")
     p.add_argument("--no-serve", action="store_true", help="default line: no serving sub-record")
+    p.add_argument("--no-hybrid", action="store_true", help="default line: no hybrid GPU + CPU sub-record")
     p.add_argument("--sub-batch-max-scale", type=int, default=14,
                    help="default line: largest R-MAT scale of the batched-launch sub-record")
     p.add_argument("--sub-serve-rate", type=float, default=0.0,
@@ -774,6 +775,35 @@ def main():
             except Exception as e:  # the baseline is reported, not required
                 ref_gpu = {"error": str(e)[-300:]}
 
+    # --- hybrid GPU + CPU execution (bb_tc.cpp:142-252): the reference's default
+    # border 0, CPU workers on the host cores beside the GPU ---
+    hybrid = None
+    if rank == 0 and world == 1 and not args.no_hybrid:
+        try:
+            workers = max(1, (os.cpu_count() or 2) - 1)
+            tl = st.task_list(sorted=True)
+            ho = options(mode="persistent", kernel="bitmap", bitmap_words=args.bitmap_words, cuda_graph=False)
+            ht, hs = [], []
+            for i in range(4):
+                t0 = time.perf_counter()
+                hc, hstat = st.count_hybrid(g.indptr, g.indices, tl, 0, workers, ho)
+                t1 = time.perf_counter()
+                assert hc == count, f"hybrid count disagrees: {hc} vs {count}"
+                if i >= 1:
+                    ht.append(t1 - t0)
+                    hs.append(hstat)
+            th = statistics.median(ht)
+            last = hs[-1]
+            hybrid = {"value": g.m / th, "unit": UNIT, "ms_per_step": th * 1e3, "border": 0, "cpu_workers": workers,
+                      "gpu_tasks": last["gpu_tasks"], "cpu_tasks": last["cpu_tasks"],
+                      "gpu_launches": last["gpu_launches"], "gpu_ms": last["gpu_ms"], "cpu_ms": last["cpu_ms"],
+                      "count_matches": True,
+                      "note": "bbtc_count_hybrid: GPU ranges through the per-task persistent queue from the head, "
+                              "CPU workers from the tail of the sorted list, wall clock, median of 3 after one "
+                              "warm-up; the host CSR's row checks are inside the time"}
+        except Exception as e:  # reported, not required
+            hybrid = {"error": str(e)[-300:]}
+
     # --- batched launch and serving sub-records (the BASELINE batching and serving configurations, short) ---
     # each in a fresh child process, as a deployment runs them (host threads and
     # device memory pools of this process do not carry over)
@@ -830,6 +860,7 @@ def main():
                               "same time" + (f"; traffic: {traffic_note}" if traffic_note else ""))},
         "cpu_baseline": cpu,
         "reference_gpu": ref_gpu,
+        "hybrid": hybrid,
         "batch": batch_rec,
         "serve": serve_rec,
         "gpu_launches": launches,

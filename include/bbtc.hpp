@@ -99,7 +99,9 @@ inline void SortTasks(std::vector<bbtc_task>& t, const BlockCSR& st) {
 }  // namespace tasks
 
 // The counting driver.  Separator keeps --border's meaning (tasks [0, b)
-// first); every task runs on the GPU.
+// first).  Every task runs on the GPU unless SetCpuWorkers adds CPU workers:
+// then tasks [0, Separator) stay on the GPU and the rest are shared, CPU
+// workers taking them from the tail (bb_tc.cpp:142-252).
 class BBTc {
  public:
   BBTc(Context& ctx, BlockCSR* st, std::vector<bbtc_task>& tasks, uint32_t P)
@@ -118,9 +120,24 @@ class BBTc {
   }
   int GetNGPU() const { return 1; }
   bbtc_opts& Options() { return opts_; }
+  // k CPU workers beside the GPU (0 = GPU only).  They read the host CSR the
+  // BlockCSR was built from; x_adj and adj must stay alive and unchanged
+  // while NoOfTriangles runs.
+  void SetCpuWorkers(uint32_t k, const std::vector<uint32_t>& x_adj, const std::vector<uint32_t>& adj) {
+    cpu_workers_ = k;
+    x_adj_ = x_adj.data();
+    adj_ = adj.data();
+  }
+  const bbtc_hybrid_stats& LastHybridStats() const { return stats_; }
 
   unsigned long long NoOfTriangles() {
     uint64_t out = 0;
+    if (cpu_workers_ > 0) {
+      const int32_t border = Separator < -2 ? -1 : Separator;
+      check(bbtc_count_hybrid(ctx_.get(), st_->get(), x_adj_, adj_, tasks_.data(), (uint32_t)tasks_.size(), border,
+                              cpu_workers_, &opts_, &out, &stats_));
+      return out;
+    }
     const int32_t border = (Separator < 0 || Separator >= (int)tasks_.size()) ? -1 : Separator;
     check(bbtc_count(ctx_.get(), st_->get(), tasks_.data(), (uint32_t)tasks_.size(), border, &opts_, &out));
     return out;
@@ -132,6 +149,10 @@ class BBTc {
   BlockCSR* st_;
   std::vector<bbtc_task> tasks_;
   bbtc_opts opts_;
+  uint32_t cpu_workers_ = 0;
+  const uint32_t* x_adj_ = nullptr;
+  const uint32_t* adj_ = nullptr;
+  bbtc_hybrid_stats stats_{};
 };
 
 }  // namespace bbtc

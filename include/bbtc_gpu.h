@@ -232,6 +232,36 @@ int bbtc_autotune(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_tune_space* space, bb
 int bbtc_count_batch(bbtc_ctx* ctx, bbtc_graph* const* graphs, uint32_t ng, const bbtc_opts* opts,
                      uint64_t* outs);
 
+/* ---- hybrid GPU + CPU execution ---------------------------------------------
+ * BBTc::NoOfTriangles with CPU workers beside the GPU (bb_tc.cpp:142-252,
+ * RunGpuKernels :142-181, RunCpuKernels :184-197; Separator from --border,
+ * bbtc.cu:54-62).  The border gives the Separator: -1 (or a value past the
+ * end) = every task on the GPU, -2 = half the list, b >= 0 = b.  Tasks
+ * [0, Separator) run on the GPU only; the rest are shared: cpu_workers host
+ * threads take them one at a time from the tail, while the GPU takes them
+ * from the head in list order, a contiguous range per bbtc_count launch, and
+ * stops at the first task a CPU worker holds.  Every task is counted once;
+ * *out is the sum.  tasks == NULL = TaskList(P) sorted heaviest first, the
+ * reference's CUDA driver order.  indptr / indices are the host CSR the graph
+ * was uploaded from (CPU workers read it; it must stay unchanged during the
+ * call; NULL is allowed when cpu_workers = 0).  CPU workers check the rows
+ * (strictly increasing, ids < n) before any of them counts: BBTC_ERR_INPUT if
+ * they break the contract.  With cpu_workers = 0 this is bbtc_count.  The
+ * context's GPU is required either way.  stats may be NULL. */
+typedef struct bbtc_hybrid_stats {
+  uint32_t gpu_tasks;    /* tasks counted on the GPU */
+  uint32_t cpu_tasks;    /* tasks counted by the CPU workers */
+  uint32_t gpu_launches; /* bbtc_count calls made by the GPU side */
+  uint32_t separator;    /* the Separator the border gave */
+  uint64_t gpu_count;    /* the GPU tasks' sum */
+  uint64_t cpu_count;    /* the CPU tasks' sum */
+  double gpu_ms;         /* wall time of the GPU side */
+  double cpu_ms;         /* wall time of the slowest CPU worker */
+} bbtc_hybrid_stats;
+int bbtc_count_hybrid(bbtc_ctx* ctx, bbtc_graph* g, const uint32_t* indptr, const uint32_t* indices,
+                      const bbtc_task* tasks, uint32_t ntasks, int32_t border, uint32_t cpu_workers,
+                      const bbtc_opts* opts, uint64_t* out, bbtc_hybrid_stats* stats);
+
 /* ---- device-side input preparation ------------------------------------------
  * The reference prepares the counting graph on the host: symmetrise, drop
  * self-loops (include/utils/utils.hpp:172-250), relabel by ascending degree
