@@ -158,7 +158,7 @@ void ParseArguments(Parameters& p, int argc, const char** argv, int devices) {
       CheckIntParams("--border", p.border, -2);
     } else if (a == "--cpu-workers") {
       p.cpu_workers = ToInt(next());
-      CheckIntParams("--cpu-workers", p.cpu_workers, -1);
+      CheckIntParams("--cpu-workers", p.cpu_workers, -2);  // bounds are strict: -1 and up
     } else if (a == "--repeat") {
       p.repeat = ToInt(next());
       CheckIntParams("--repeat", p.repeat);

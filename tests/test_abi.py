@@ -95,6 +95,8 @@ int main() {
   try { bbtc::Context ctx(0); } catch (const bbtc::Error& e) { ctx_status = e.status(); }
   try { bbtc::tasks::TaskList(65); } catch (const bbtc::Error& e) { list_status = e.status(); }
   std::printf("%d %d %zu\n", ctx_status, list_status, bbtc::tasks::TaskList(4).size());
+  (void)&bbtc::BBTc::SetCpuWorkers;  // the hybrid methods compile
+  (void)&bbtc::BBTc::LastHybridStats;
   return 0;
 }
 """)
@@ -122,7 +124,7 @@ def test_struct_layouts_match_the_header(tmp_path):
     mirrors = {"bbtc_task": core.Task, "bbtc_opts": core.Opts, "bbtc_graph_info": core.GraphInfo,
                "bbtc_tune_space": autotune.TuneSpace, "bbtc_csr_dev": core.CsrDev,
                "bbtc_server_opts": core.ServerOpts, "bbtc_request_info": core.RequestInfo,
-               "bbtc_server_stats": core.ServerStats}
+               "bbtc_server_stats": core.ServerStats, "bbtc_hybrid_stats": core.HybridStats}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "bbtc_gpu.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')

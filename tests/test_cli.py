@@ -44,3 +44,16 @@ def test_range_checks(tmp_path):
     assert "--repeat has to be set in between: 0 < --repeat" in run("--graph", str(g), "--repeat", "0").stdout
     assert "--border has to be set in between: -2 < --border" in run("--graph", str(g), "--border", "-3").stdout
     assert "Wrong partitioning algorithm." in run("--graph", str(g), "--partitioner", "xyz").stdout
+
+
+def test_cpu_workers_flag_bounds(tmp_path):
+    """--cpu-workers (not in the reference) takes -1 (the reference's split of
+    OpenMP threads) and up; below that the range message and usage, exit 0."""
+    g = tmp_path / "g.el"
+    g.write_text("0 1\n")
+    r = run("--graph", str(g), "--cpu-workers", "-2")
+    assert "--cpu-workers has to be set in between: -2 < --cpu-workers" in r.stdout and r.returncode == 0
+    assert "--cpu-workers <int>" in run("--help").stdout
+    for v in ("-1", "0", "6"):
+        r = run("--graph", str(g), "--cpu-workers", v, "--border", "3")
+        assert "has to be set in between" not in r.stdout, v
