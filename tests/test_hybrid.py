@@ -122,14 +122,14 @@ def test_claim_protocol_counts_every_task_once(harness, case):
 
 
 def test_cpu_takes_the_tail_when_the_gpu_is_slow(harness):
-    """With a slow GPU side and Separator 0, CPU workers count part of the list,
-    all of it at the tail: the GPU's tasks are a prefix of the list."""
+    """With a slow GPU side, CPU workers count part of the shared list (the
+    Separator is 1, so the GPU side launches at least once)."""
     exe, d = harness
     g0 = graphs.rmat(9, 8, seed=1)
     cuts = graphs.cuts(g0, 8, "uni")
     tasks = task_list(8)
     g, t = write(d, "slow", g0.n, g0.indptr, g0.indices, cuts, tasks)
-    out = run(exe, g, t, "run", 0, 4, 5000, 0)
+    out = run(exe, g, t, "run", 1, 4, 5000, 0)
     rc, total, gt, ct, launches, sep, gc, cc = (int(x) for x in out[0].split())
     assert rc == 0 and total == oracle.count(g0.n, g0.indptr, g0.indices, cuts)
     assert ct > 0 and gt > 0 and launches >= 1
@@ -159,13 +159,16 @@ def test_rows_breaking_the_contract_void_the_count(harness):
 
 
 def test_gpu_failure_stops_the_workers(harness):
+    """A failing GPU launch is the call's status, and nothing is summed.  The
+    border keeps tasks for the GPU, so it launches at least once (with
+    border 0, fast CPU workers may take every task before it starts)."""
     exe, d = harness
     g0 = graphs.rmat(9, 8, seed=1)
     cuts = graphs.cuts(g0, 6, "uni")
     tasks = task_list(6)
     g, t = write(d, "gfail", g0.n, g0.indptr, g0.indices, cuts, tasks)
     for workers in (0, 2):
-        out = run(exe, g, t, "run", 0, workers, 0, 1)
+        out = run(exe, g, t, "run", 5, workers, 0, 1)
         rc, total = (int(x) for x in out[0].split()[:2])
         assert rc == -2 and total == 0
 
