@@ -804,7 +804,7 @@ def main():
         except Exception as e:  # reported, not required
             hybrid = {"error": str(e)[-300:]}
 
-    # --- batched launch and serving sub-records (the BASELINE batching and serving configurations, short) ---
+    # --- batched launch and serving sub-records (576 graphs in one launch; Poisson request streams; short) ---
     # each in a fresh child process, as a deployment runs them (host threads and
     # device memory pools of this process do not carry over)
     batch_rec = serve_rec = None
