@@ -410,7 +410,7 @@ class BBTc:
         if self._cpu > 0:
             sep = -1 if self.Separator is None else int(self.Separator)
             count, self.last_stats = self.st.count_hybrid(self._host[0], self._host[1], self.tasks,
-                                                          max(sep, -2), self._cpu, self.opts)
+                                                          sep if sep >= -2 else -1, self._cpu, self.opts)
             return count
         border = -1 if self.Separator is None or self.Separator < 0 or self.Separator >= len(self.tasks) \
             else int(self.Separator)
