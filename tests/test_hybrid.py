@@ -70,6 +70,9 @@ def cases():
     yield "chunglu-uni7", g.n, g.indptr, g.indices, graphs.cuts(g, 7, "uni")
     ip, ix = unoriented(300, 3)
     yield "unoriented-4", 300, ip, ix, np.array([0, 60, 61, 200, 301], np.uint32)  # phantom row past n
+    yield "edgeless-3", 40, np.zeros(41, np.uint32), np.zeros(0, np.uint32), np.array([0, 10, 10, 40], np.uint32)
+    g = graphs.rmat(8, 8, seed=3)
+    yield "rmat8-one-part", g.n, g.indptr, g.indices, np.array([0, g.n + 1], np.uint32)
 
 
 @pytest.mark.parametrize("case", list(cases()), ids=lambda c: c[0])
