@@ -86,8 +86,9 @@ extern "C" int bbtc_count_hybrid(bbtc_ctx* ctx, bbtc_graph* g, const uint32_t* i
     return counters[w].count(hc, part[3 * (size_t)t], part[3 * (size_t)t + 1], part[3 * (size_t)t + 2]);
   };
   auto prepare = [&](uint32_t w) -> bool {
-    const uint64_t lo = (uint64_t)hc.n * w / cpu_workers, hi = (uint64_t)hc.n * (w + 1) / cpu_workers;
-    return bbtc::hybrid::check_rows(hc, (uint32_t)lo, (uint32_t)hi);
+    uint32_t lo, hi;
+    bbtc::hybrid::row_share(hc, w, cpu_workers, &lo, &hi);
+    return bbtc::hybrid::check_rows(hc, lo, hi);
   };
 
   bbtc::hybrid::Stats s;

@@ -77,6 +77,21 @@ inline bool check_rows(const HostCsr& g, uint32_t lo, uint32_t hi) {
   return true;
 }
 
+// Rows [*lo, *hi) of worker w of W: contiguous, about m / W entries each
+// (R-MAT rows are skewed, so equal row counts would not balance the checks).
+inline void row_share(const HostCsr& g, uint32_t w, uint32_t W, uint32_t* lo, uint32_t* hi) {
+  auto first_row_at = [&](uint32_t part) -> uint32_t {
+    if (part == 0) return 0;
+    if (part >= W) return g.n;
+    const uint64_t e = g.m * part / W;
+    return (uint32_t)(std::lower_bound(g.indptr, g.indptr + g.n + 1, e,
+                                       [](uint32_t a, uint64_t b) { return (uint64_t)a < b; }) - g.indptr);
+  };
+  *lo = std::min(first_row_at(w), g.n);
+  *hi = std::min(first_row_at(w + 1), g.n);
+  if (w + 1 == W) *hi = g.n;
+}
+
 // Widest part, clipped to the rows that exist.
 inline uint32_t widest_part(const HostCsr& g) {
   uint32_t w = 0;

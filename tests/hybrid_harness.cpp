@@ -115,8 +115,9 @@ int main(int argc, char** argv) {
     return cpu_tc[w].count(g, i, j, k);
   };
   auto prepare = [&](uint32_t w) -> bool {
-    const uint64_t lo = (uint64_t)n * w / workers, hi = (uint64_t)n * (w + 1) / workers;
-    return check_rows(g, (uint32_t)lo, (uint32_t)hi);
+    uint32_t lo, hi;
+    row_share(g, w, workers, &lo, &hi);
+    return check_rows(g, lo, hi);
   };
   Stats s;
   uint64_t out = 0;

@@ -146,19 +146,24 @@ def test_rows_breaking_the_contract_void_the_count(harness):
     g0 = graphs.rmat(9, 8, seed=1)
     cuts = graphs.cuts(g0, 4, "uni")
     tasks = task_list(4)
-    long_row = int(np.argmax(np.diff(g0.indptr)))
-    for kind in ("unsorted", "id"):
-        ix = g0.indices.copy()
-        s = int(g0.indptr[long_row])
-        if kind == "unsorted":
-            ix[s], ix[s + 1] = ix[s + 1], ix[s]
-        else:
-            ix[int(g0.indptr[long_row + 1]) - 1] = g0.n
-        g, t = write(d, "bad-" + kind, g0.n, g0.indptr, ix, cuts, tasks)
-        assert run(exe, g, t, "tasks")[0] == "rows"
-        out = run(exe, g, t, "run", 0, 3, 0, 0)
-        rc, total, gt, ct = (int(x) for x in out[0].split()[:4])
-        assert rc == -4 and total == 0 and ct == 0, kind
+    deg = np.diff(g0.indptr.astype(np.int64))
+    wide = np.nonzero(deg >= 2)[0]
+    # the longest row and the first and last rows with two ids: the workers'
+    # row shares (split by entries) must cover every row
+    for row in (int(np.argmax(deg)), int(wide[0]), int(wide[-1])):
+        for kind in ("unsorted", "id"):
+            ix = g0.indices.copy()
+            s = int(g0.indptr[row])
+            if kind == "unsorted":
+                ix[s], ix[s + 1] = ix[s + 1], ix[s]
+            else:
+                ix[int(g0.indptr[row + 1]) - 1] = g0.n
+            g, t = write(d, f"bad-{kind}-{row}", g0.n, g0.indptr, ix, cuts, tasks)
+            assert run(exe, g, t, "tasks")[0] == "rows"
+            for workers in (1, 3, 7):
+                out = run(exe, g, t, "run", 0, workers, 0, 0)
+                rc, total, gt, ct = (int(x) for x in out[0].split()[:4])
+                assert rc == -4 and total == 0 and ct == 0, (kind, row, workers)
 
 
 def test_gpu_failure_stops_the_workers(harness):
