@@ -190,7 +190,8 @@ void bbtc_opts_default(bbtc_opts* o);
  * tasks == NULL counts the whole TaskList(P) (sorted per opts->sort_tasks).
  * border follows --border (utils.hpp:111-114, bbtc.cu:54-62): -1 = every task
  * on the GPU; b >= 0 = tasks [0, b) are queued first, then the rest; all on
- * the GPU (there are no CPU workers).  *out receives the exact count.
+ * the GPU (CPU workers beside it: bbtc_count_hybrid).  *out receives the
+ * exact count.
  * Replaces BBTc::NoOfTriangles (bb_tc.cpp:200-252). */
 int bbtc_count(bbtc_ctx* ctx, bbtc_graph* g, const bbtc_task* tasks, uint32_t ntasks, int32_t border,
                const bbtc_opts* opts, uint64_t* out);
