@@ -13,6 +13,7 @@
  *   - tasks::TaskList / tasks::SortTasks include/utils/tasks.hpp:7-34
  *   - DenseKernel / SparseKernel launch  src/triangle_counting/bb_tc.cpp:76-115
  *   - BBTc::NoOfTriangles                src/triangle_counting/bb_tc.cpp:200-252
+ *   - RunGpuKernels / RunCpuKernels      src/triangle_counting/bb_tc.cpp:142-197 (hybrid)
  * Threading: a context and the graphs made with it belong to one host thread
  * at a time (the reference drives BBTc from the main thread, src/bbtc.cu:40-89);
  * the request server (bbtc_server_*) is safe to call from any thread.
