@@ -78,9 +78,13 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-threads", type=int, default=0)
-    p.add_argument("--config", default="single", choices=["single", "batch", "serve"],
+    p.add_argument("--config", default="single", choices=["single", "batch", "serve", "hybrid"],
                    help="single: one R-MAT s22 graph (default); batch: 512 R-MAT + 64 RGG graphs in one "
-                        "launch; serve: Poisson request stream through the continuous-batching server")
+                        "launch; serve: Poisson request stream through the continuous-batching server; "
+                        "hybrid: the graph counted by the GPU and CPU workers together (bbtc_count_hybrid)")
+    p.add_argument("--border", type=int, default=0, help="hybrid: the reference's --border (default 0)")
+    p.add_argument("--cpu-workers", type=int, default=0,
+                   help="hybrid: CPU worker threads (0: one per host core but one)")
     p.add_argument("--batch-max-scale", type=int, default=20)
     p.add_argument("--batch-plain-steps", type=int, default=-1,
                    help="batch: steps of the one-launch-per-task comparison (-1: steps / 2, at least 2)")
@@ -406,6 +410,43 @@ def run_batch(args):
     print(json.dumps(res), flush=True)
 
 
+def run_hybrid(args):
+    """bbtc_count_hybrid on one graph: the reference's default border 0, one CPU
+    worker per host core but one beside the GPU; wall clock per call, the
+    host CSR's row checks included."""
+    from bbtc_b200 import Context, Graph, options
+    ctx = Context(0)
+    g, cuts, _ = make_graph(args, args.seed)
+    st = Graph.from_csr(ctx, g, cuts)
+    want = st.count()
+    workers = args.cpu_workers if args.cpu_workers > 0 else max(1, (os.cpu_count() or 2) - 1)
+    tl = st.task_list(sorted=True)
+    ho = options(mode="persistent", kernel="bitmap", bitmap_words=args.bitmap_words, cuda_graph=False)
+    ht, hs = [], []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        hc, hstat = st.count_hybrid(g.indptr, g.indices, tl, args.border, workers, ho)
+        t1 = time.perf_counter()
+        assert hc == want, f"hybrid count disagrees: {hc} vs {want}"
+        if i >= args.warmup:
+            ht.append(t1 - t0)
+            hs.append(hstat)
+    th = statistics.median(ht)
+    st.free()
+    ctx.close()
+    res = {"metric": METRIC, "value": g.m / th, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": th * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+           "config": {"workload": f"hybrid: {workload_name(args)} {args.partitioner} ncut {args.ncut}",
+                      "border": args.border, "cpu_workers": workers, "triangles": want,
+                      "gpu_side": "per-task persistent queue (bitmap kernel) over contiguous ranges from the head"},
+           "splits": [{k: h[k] for k in ("gpu_tasks", "cpu_tasks", "gpu_launches", "separator")} for h in hs],
+           "gpu_ms": [h["gpu_ms"] for h in hs], "cpu_ms": [h["cpu_ms"] for h in hs],
+           "note": "wall clock of bbtc_count_hybrid (CPU workers from the tail of the sorted list, the GPU from "
+                   "the head), median over the steps; every count equal to the GPU-only count"}
+    print(json.dumps(res), flush=True)
+
+
 def serve_pool(max_scale: int, pin: bool):
     """Request graphs: R-MAT scale 12 + Geom(0.3) truncated at max_scale, edge
     factor 16; a pool of distinct seeds per scale (fewer for the big ones).
@@ -587,6 +628,8 @@ def main():
         return run_batch(args)
     if args.config == "serve":
         return run_serve(args)
+    if args.config == "hybrid":
+        return run_hybrid(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -775,34 +818,15 @@ def main():
             except Exception as e:  # the baseline is reported, not required
                 ref_gpu = {"error": str(e)[-300:]}
 
-    # --- hybrid GPU + CPU execution (bb_tc.cpp:142-252): the reference's default
-    # border 0, CPU workers on the host cores beside the GPU ---
+    # --- hybrid GPU + CPU execution (bb_tc.cpp:142-252) on the same graph, in a
+    # child process (its CPU worker threads and their memory stay out of this one) ---
     hybrid = None
     if rank == 0 and world == 1 and not args.no_hybrid:
-        try:
-            workers = max(1, (os.cpu_count() or 2) - 1)
-            tl = st.task_list(sorted=True)
-            ho = options(mode="persistent", kernel="bitmap", bitmap_words=args.bitmap_words, cuda_graph=False)
-            ht, hs = [], []
-            for i in range(4):
-                t0 = time.perf_counter()
-                hc, hstat = st.count_hybrid(g.indptr, g.indices, tl, 0, workers, ho)
-                t1 = time.perf_counter()
-                assert hc == count, f"hybrid count disagrees: {hc} vs {count}"
-                if i >= 1:
-                    ht.append(t1 - t0)
-                    hs.append(hstat)
-            th = statistics.median(ht)
-            last = hs[-1]
-            hybrid = {"value": g.m / th, "unit": UNIT, "ms_per_step": th * 1e3, "border": 0, "cpu_workers": workers,
-                      "gpu_tasks": last["gpu_tasks"], "cpu_tasks": last["cpu_tasks"],
-                      "gpu_launches": last["gpu_launches"], "gpu_ms": last["gpu_ms"], "cpu_ms": last["cpu_ms"],
-                      "count_matches": True,
-                      "note": "bbtc_count_hybrid: GPU ranges through the per-task persistent queue from the head, "
-                              "CPU workers from the tail of the sorted list, wall clock, median of 3 after one "
-                              "warm-up; the host CSR's row checks are inside the time"}
-        except Exception as e:  # reported, not required
-            hybrid = {"error": str(e)[-300:]}
+        hybrid = child_line(["--config", "hybrid", "--family", args.family, "--scale", str(args.scale),
+                             "--edge-factor", str(args.edge_factor), "--seed", str(args.seed), "--ncut",
+                             str(args.ncut), "--partitioner", args.partitioner, "--steps", "3", "--warmup", "1"])
+        if hybrid is not None and "error" not in hybrid:
+            hybrid["count_matches"] = hybrid.get("config", {}).get("triangles") == count
 
     # --- batched launch and serving sub-records (576 graphs in one launch; Poisson request streams; short) ---
     # each in a fresh child process, as a deployment runs them (host threads and
