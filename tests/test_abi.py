@@ -59,6 +59,9 @@ def test_errors_are_status_codes_not_crashes():
     assert lib.bbtc_task_list(65, None, 0, ctypes.byref(ctypes.c_uint32())) == -1
     assert lib.bbtc_graph_upload(None, 0, None, None, 0, None, 0, None) == -1
     assert lib.bbtc_count(None, None, None, 0, -1, None, None) == -1
+    out = ctypes.c_uint64()
+    assert lib.bbtc_count_hybrid(None, None, None, None, None, 0, 0, 2, None, ctypes.byref(out), None) == -1
+    assert "NULL" in core.last_error()
 
 
 def test_allocation_fault_hook_arms_and_disarms():
