@@ -9,7 +9,8 @@
 //       runs the protocol; the stand-in GPU sleeps gpu_us per task of each
 //       launch and returns BBTC_ERR_CUDA (-2) on launch number gpu_fail_call
 //       (0 = never).  Prints "rc out gpu_tasks cpu_tasks gpu_launches sep
-//       gpu_count cpu_count", then per task how often it was counted.
+//       gpu_count cpu_count", then per task how often it was counted and by
+//       which side ("<times> G" or "<times> C").
 // graph file: uint32 n, uint32 P, uint64 m, indptr[n+1], indices[m], cuts[P+1]
 // tasks file: uint32 ntasks, then ntasks x (ab, bc, ac) uint32
 #include <atomic>
@@ -92,7 +93,11 @@ int main(int argc, char** argv) {
   const int fail_call = std::atoi(argv[7]);
 
   std::unique_ptr<std::atomic<uint32_t>[]> seen(new std::atomic<uint32_t>[nt ? nt : 1]);
-  for (uint32_t t = 0; t < nt; t++) seen[t].store(0);
+  std::unique_ptr<std::atomic<char>[]> side(new std::atomic<char>[nt ? nt : 1]);
+  for (uint32_t t = 0; t < nt; t++) {
+    seen[t].store(0);
+    side[t].store('-');
+  }
   TaskCounter gpu_tc(width);
   std::vector<TaskCounter> cpu_tc(workers, TaskCounter(width));
   int calls = 0;
@@ -104,6 +109,7 @@ int main(int argc, char** argv) {
       ijk(t, &i, &j, &k);
       *c += gpu_tc.count(g, i, j, k);
       seen[t].fetch_add(1);
+      side[t].store('G');
       if (gpu_us) std::this_thread::sleep_for(std::chrono::microseconds(gpu_us));
     }
     return 0;
@@ -112,6 +118,7 @@ int main(int argc, char** argv) {
     uint32_t i, j, k;
     ijk(t, &i, &j, &k);
     seen[t].fetch_add(1);
+    side[t].store('C');
     return cpu_tc[w].count(g, i, j, k);
   };
   auto prepare = [&](uint32_t w) -> bool {
@@ -125,6 +132,6 @@ int main(int argc, char** argv) {
   const int rc = run(nt, sep, workers, gpu, cpu, prepare, -4, -3, &out, &s);
   std::printf("%d %llu %u %u %u %u %llu %llu\n", rc, (unsigned long long)out, s.gpu_tasks, s.cpu_tasks,
               s.gpu_launches, sep, (unsigned long long)s.gpu_count, (unsigned long long)s.cpu_count);
-  for (uint32_t t = 0; t < nt; t++) std::printf("%u\n", seen[t].load());
+  for (uint32_t t = 0; t < nt; t++) std::printf("%u %c\n", seen[t].load(), side[t].load());
   return 0;
 }

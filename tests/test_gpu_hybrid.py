@@ -41,6 +41,9 @@ def test_hybrid_counts_equal_oracle(ctx, case):
     try:
         tasks = st.task_list(sorted=True)
         nt = len(tasks)
+        # each side's sum against the oracle's task sums: the GPU counts the
+        # list's first gpu_tasks positions, the CPU workers the rest
+        per_task = [oracle.task_count(n, ip, ix, cuts, int(t["ab"]), int(t["bc"]), int(t["ac"])) for t in tasks]
         for border in (-1, -2, 0, 7, nt + 1):
             for workers in (0, 2, 6):
                 for mode in ("persistent", "plain"):
@@ -49,6 +52,8 @@ def test_hybrid_counts_equal_oracle(ctx, case):
                     assert got == want, key
                     assert s["gpu_count"] + s["cpu_count"] == want, key
                     assert s["gpu_tasks"] + s["cpu_tasks"] == nt, key
+                    assert s["gpu_count"] == sum(per_task[:s["gpu_tasks"]]), key
+                    assert s["cpu_count"] == sum(per_task[s["gpu_tasks"]:]), key
                     sep = nt if border in (-1, nt + 1) else nt // 2 if border == -2 else border
                     assert s["separator"] == sep and s["gpu_tasks"] >= sep, key
                     if workers == 0 or sep == nt:

@@ -111,8 +111,11 @@ def test_claim_protocol_counts_every_task_once(harness, case):
             for gpu_us in (0, 300):
                 out = run(exe, g, t, "run", border, workers, gpu_us, 0)
                 rc, total, gt, ct, launches, sep, gc, cc = (int(x) for x in out[0].split())
-                seen = [int(x) for x in out[1:] if x]
+                seen = [int(x.split()[0]) for x in out[1:] if x]
+                sides = "".join(x.split()[1] for x in out[1:] if x)
                 key = (border, workers, gpu_us)
+                # the GPU's tasks are the list's first gt positions, the CPU's the rest
+                assert sides == "G" * gt + "C" * ct, key
                 assert rc == 0, key
                 assert total == want and gc + cc == want, key
                 assert seen == [1] * nt, key
@@ -136,7 +139,7 @@ def test_cpu_takes_the_tail_when_the_gpu_is_slow(harness):
     rc, total, gt, ct, launches, sep, gc, cc = (int(x) for x in out[0].split())
     assert rc == 0 and total == oracle.count(g0.n, g0.indptr, g0.indices, cuts)
     assert ct > 0 and gt > 0 and launches >= 1
-    assert [int(x) for x in out[1:] if x] == [1] * len(tasks)
+    assert [x for x in out[1:] if x] == ["1 G"] * gt + ["1 C"] * ct
 
 
 def test_rows_breaking_the_contract_void_the_count(harness):
