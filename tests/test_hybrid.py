@@ -3,7 +3,7 @@ the CPU: the CPU workers' task count against the oracle's task sum, and the
 claim protocol of bb_tc.cpp:142-252 (GPU from the head up to the first task a
 CPU worker holds, CPU workers from the tail down to the Separator) with a
 stand-in for the GPU side.  The GPU side itself is tested in
-tests/test_gpu_hybrid.py."""
+tests/test_gpu_with_cpu_workers.py."""
 import os
 import shutil
 import subprocess
