@@ -197,3 +197,34 @@ def test_shape_checks(harness):
     short[-1] = g0.n - 1  # cuts[P] < n
     g, t = write(d, "shape2", g0.n, g0.indptr, g0.indices, short, task_list(3))
     assert run(exe, g, t, "tasks")[0] == "shape"
+
+
+def test_claim_protocol_under_thread_sanitizer(tmp_path):
+    """The claim protocol's shared state (tail counter, claim flags, the CPU
+    workers' start barrier, sums) has no data race: the harness built with
+    ThreadSanitizer, over borders, worker counts, GPU speeds and a failing
+    GPU launch, reports nothing."""
+    cxx = shutil.which("g++") or shutil.which("c++")
+    exe = tmp_path / "harness_tsan"
+    r = subprocess.run([cxx, "-std=c++17", "-O1", "-g", "-fsanitize=thread", "-pthread", "-I",
+                        os.path.join(ROOT, "bbtc_b200", "csrc"), os.path.join(ROOT, "tests", "hybrid_harness.cpp"),
+                        "-o", str(exe)], capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.skip("no ThreadSanitizer in this compiler: " + r.stderr[-200:])
+    g0 = graphs.rmat(9, 16, seed=2)
+    cuts = graphs.cuts(g0, 8, "pal")
+    tasks = task_list(8)[np.random.default_rng(1).permutation(120)]
+    g, t = write(tmp_path, "tsan", g0.n, g0.indptr, g0.indices, cuts, tasks)
+    want = oracle.count(g0.n, g0.indptr, g0.indices, cuts)
+    for border in (0, 7, -2):
+        for workers in (1, 6):
+            for gpu_us, fail in ((0, 0), (200, 0), (0, 1)):
+                b = max(border, 1) if fail and border >= 0 else border  # a GPU region: the GPU side launches
+                r = subprocess.run([str(exe), str(g), str(t), "run", str(b), str(workers), str(gpu_us),
+                                    str(fail)], capture_output=True, text=True, timeout=300)
+                if "unexpected memory mapping" in r.stderr:
+                    pytest.skip("ThreadSanitizer cannot run on this kernel's address layout")
+                key = (border, workers, gpu_us, fail)
+                assert r.returncode == 0 and "ThreadSanitizer" not in r.stderr, (key, r.stderr[:3000])
+                rc, total = (int(x) for x in r.stdout.split()[:2])
+                assert (rc, total) == ((-2, 0) if fail else (0, want)), key
