@@ -93,7 +93,10 @@ extern "C" int bbtc_count_hybrid(bbtc_ctx* ctx, bbtc_graph* g, const uint32_t* i
 
   bbtc::hybrid::Stats s;
   const uint32_t sep = bbtc::hybrid::separator(border, nt);
-  const int rc = bbtc::hybrid::run(nt, sep, cpu_workers, gpu, cpu, prepare, BBTC_ERR_INPUT, BBTC_ERR_NOMEM, out, &s);
+  // distinct codes for the protocol's own failures, so that a status the GPU
+  // side returned (and its message) passes through unchanged
+  constexpr int kBadRows = -1001, kNoThreads = -1002;
+  const int rc = bbtc::hybrid::run(nt, sep, cpu_workers, gpu, cpu, prepare, kBadRows, kNoThreads, out, &s);
   if (stats) {
     stats->gpu_tasks = s.gpu_tasks;
     stats->cpu_tasks = s.cpu_tasks;
@@ -104,7 +107,7 @@ extern "C" int bbtc_count_hybrid(bbtc_ctx* ctx, bbtc_graph* g, const uint32_t* i
     stats->gpu_ms = s.gpu_ms;
     stats->cpu_ms = s.cpu_ms;
   }
-  if (rc == BBTC_ERR_INPUT) return fail(BBTC_ERR_INPUT, "host CSR breaks the input contract (row not strictly increasing or id >= n)");
-  if (rc == BBTC_ERR_NOMEM) return fail(BBTC_ERR_NOMEM, "CPU worker threads could not be started");
-  return rc;  // a failing bbtc_count has set the message
+  if (rc == kBadRows) return fail(BBTC_ERR_INPUT, "host CSR breaks the input contract (row not strictly increasing or id >= n)");
+  if (rc == kNoThreads) return fail(BBTC_ERR_NOMEM, "CPU worker threads could not be started");
+  return rc;  // 0, or a failing bbtc_count's status (it has set the message)
 }
